@@ -1,0 +1,172 @@
+/*
+ * viss.h -- C ABI of the B200 (sm_100a) visibility / imaging library.
+ *
+ * The reference (SSshuishui/viss_optimize_3d) has no library: its hot path is
+ * a set of __global__ kernels driven by one host function per executable.
+ * Each entry point below replaces one of those kernels or host stages; the
+ * comment before it names the reference file:line it stands in for.
+ *
+ * Conventions
+ *   - Every function returns an int status (VISS_OK == 0, negative on error)
+ *     instead of the reference's CHECK -> exit(1) (error.cuh:4-19).  The text
+ *     of the last failure on the calling thread is in viss_last_error().
+ *   - Array arguments are DEVICE pointers owned by the caller unless the name
+ *     says host_.  No function frees or keeps a caller pointer beyond the call
+ *     (plans copy what they keep).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls are asynchronous on that stream unless stated.
+ *   - Complex arrays are interleaved (re, im) pairs.
+ *   - Sky directions are the reference's (l, m, n) (vissgen3d_blockage.cu:
+ *     53-74): l = sin(theta)cos(phi), m = -sin(theta)sin(phi), n = cos(theta)
+ *     for a HEALPix (theta, phi).
+ *   - A plan may be used from one stream at a time.
+ */
+#ifndef VISS_H
+#define VISS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define VISS_OK 0
+#define VISS_ERR_ARG (-1)       /* bad argument: NULL pointer, size out of range */
+#define VISS_ERR_CUDA (-2)      /* CUDA runtime error (text in viss_last_error) */
+#define VISS_ERR_ALLOC (-3)     /* device workspace allocation failed */
+#define VISS_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up */
+#define VISS_ERR_NOTFINITE (-5) /* NaN/inf in an input that must be finite */
+#define VISS_ERR_IO (-6)        /* file missing or malformed (host drivers) */
+#define VISS_ERR_STATE (-7)     /* plan used before the data it needs was set */
+
+/* ------------------------------------------------------------------- flags */
+#define VISS_FP64 0x1        /* plain FP64 path: FP64 sincos and sums */
+#define VISS_NO_MASK 0x2     /* ignore occultation references */
+#define VISS_NO_OFFSET 0x4   /* ignore the per-sample phase offset */
+#define VISS_ACCUMULATE 0x8  /* add into the output instead of overwriting */
+
+/* HEALPix schemes */
+#define VISS_RING 0
+#define VISS_NESTED 1
+
+typedef struct viss_plan viss_plan;
+
+int viss_version(void);
+const char *viss_status_string(int status);
+/* Copies the last error message of the calling thread into buf (always NUL
+ * terminated when len > 0); returns the full message length. */
+size_t viss_last_error(char *buf, size_t len);
+
+/* ------------------------------------------------------------ HEALPix tables
+ * Replaces pix2ang.cu:61-88 (mk_pix2xy): the 1024-entry bit de-interleave
+ * tables (x = even bits, y = odd bits of a 10-bit index). Device int32[1024]. */
+int viss_mk_pix2xy(int32_t *pix2x, int32_t *pix2y, void *stream);
+
+/* Replaces pix2ang.cu:92-160 (f_pix2and_nest) and its RING twin: FP64
+ * colatitude theta, longitude phi in [0, 2pi) and the HEALPix unit vector
+ * (x, y, z) (count x 3) of pixels [first, first+count) in `scheme`.
+ * Any of theta / phi / xyz may be NULL. */
+int viss_pix2ang(int nside, int scheme, int64_t first, int64_t count, double *theta,
+                 double *phi, double *xyz, void *stream);
+
+/* Index permutation between schemes: out[p] = index in `to_scheme` of pixel p
+ * of `from_scheme` (nest2ring / ring2nest), p in [0, 12 nside^2). int64. */
+int viss_pix_convert(int nside, int from_scheme, int to_scheme, int64_t *out, void *stream);
+
+/* Sky directions (l, m, n) = (x, -y, z) of the HEALPix unit vectors, FP64,
+ * npix x 3 (the convention of vissgen3d_blockage.cu:53-74). */
+int viss_pix2lmn(int nside, int scheme, double *lmn, void *stream);
+
+/* ---------------------------------------------------- drop-in sky pre-pass
+ * Replaces healpix_moonback_pre (vissgen3d_blockage.cu:53-74) for FP32 text
+ * inputs: lmn (npix x 3, FP64) from FP32 theta/phi with the reference's angle
+ * edits, and B_out = B * s.  B_out may alias B. */
+int viss_sky_pre(int64_t npix, const float *theta, const float *phi, const float *B, float s,
+                 double *lmn, float *B_out, void *stream);
+
+/* ------------------------------------------------------------- occulters
+ * Occulter table row (qx, qy, qz, thr): direction s is visible iff
+ * fma(s2,q2, fma(s1,q1, s0*q0)) >= thr  (vissgen3d_blockage.cu:88-94).
+ * From satellite positions P (n x 3, metres from the Moon's centre):
+ *   mode 0: ray-sphere test against a Moon of radius R: thr = -sqrt(1-(R/|P|)^2)
+ *   mode 1: the reference's fixed cone: thr = fixed_thr
+ * occ is n x 4 FP64.  viss_cone_threshold gives the reference's fixed_thr
+ * (vissgen3d_blockage.cu:249-252: cos(pi - asinf(R/(R+h))), host FP32 asinf). */
+int viss_occulters(int64_t n, const double *P, double R, int mode, double fixed_thr,
+                   double *occ, void *stream);
+double viss_cone_threshold(float R, float h);
+
+/* Mask bits for testing: bit j of row k set iff (sample k, pixel j) is
+ * visible under refs (K x 3 int32 rows into occ; -1 = unused).  bits is
+ * K x ceil(J/32) uint32. */
+int viss_mask_bits(int64_t K, int64_t J, const double *lmn, const int32_t *refs,
+                   const double *occ, uint32_t *bits, void *stream);
+
+/* ------------------------------------------------------------------ plans
+ * A plan holds the pixel and sample geometry in the kernels' staging layout,
+ * the tile bounding cones used to skip / fast-path occultation, the cross-
+ * block partial-sum workspace and the tuned launch shapes. */
+int viss_plan_create(viss_plan **plan);
+int viss_plan_destroy(viss_plan *plan);
+
+/* Pixel directions lmn (J x 3 FP64, device). */
+int viss_plan_set_pixels(viss_plan *plan, int64_t J, const double *lmn, void *stream);
+
+/* Samples: uvw (K x 3 FP64 in wavelengths), off (K FP64 turns, or NULL),
+ * refs (K x 3 int32 into occ, or NULL = never occulted), occ (G x 4 FP64). */
+int viss_plan_set_samples(viss_plan *plan, int64_t K, const double *uvw, const double *off,
+                          const int32_t *refs, int64_t G, const double *occ, void *stream);
+
+/* Forward visibilities, replaces healpix_moonback_viss
+ * (vissgen3d_blockage.cu:76-102):
+ *   V_k = sum_j sky_j vis_kj exp(-2 pi i (u_k . s_j + off_k)),  k < K
+ * sky: J FP32; V: K complex64.  Split precision by default (FP64 phase and
+ * turn reduction, FP32 sincos, compensated FP32 sums, FP64 cross-block sum);
+ * VISS_FP64 selects the plain FP64 path. */
+int viss_forward(viss_plan *plan, const float *sky, float *V, int flags, void *stream);
+
+/* Imaging adjoint, replaces computeC (vissgen3d_blockage.cu:167-192):
+ *   image_j = scale * sum_k Re(coef_k exp(+2 pi i (u_k . s_j + off_k))) vis_kj
+ * coef: K complex64 (the weighted visibilities w_k V_k); image: J FP32. */
+int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, int flags,
+                 void *stream);
+
+/* Terms evaluated by the last viss_forward / viss_adjoint on this plan
+ * (visible-or-mixed pairs actually exponentiated) and the total K*J, read
+ * back from the device (synchronises the plan's last stream). */
+int viss_plan_last_counts(viss_plan *plan, int64_t *evaluated, int64_t *total);
+
+/* ----------------------------------------------- density compensation
+ * Replaces ceilAndScale + countOccurrences + calculateR + calculateDcf
+ * (vissgen3d_blockage.cu:105-141; the un-shifted formula of
+ * vissgen3d_noblockage.cu:132-141):
+ *   gs_i = ceil((bll_i - 1/4) / 0.5)  (FP32, as the reference)
+ *   counts[p-1] = multiplicity * #{i : gs_i == p}, p in [1, nr]  (uint32)
+ *   dcf[0] = 1/(4 pi); dcf[k] = (2 pi/3)(R^3 - (R-1/2)^3) / counts[k-1],
+ *   R = k/2 + 1/4 (FP64, stored FP32).  gs / counts may be NULL. */
+int viss_dcf(int64_t n, const float *bll, int nr, int multiplicity, int32_t *gs,
+             uint32_t *counts, float *dcf, void *stream);
+
+/* Replaces viss_gamma_trans (vissgen3d_blockage.cu:144-164), weights part:
+ *   dg_i = 1.5 sqrt|1 - 4x^2| / sqrt(1 - x^2), x = w_i / bll_i (|x|>=1: inf)
+ *   wt_i = min(dcf[clamp(gs_i, 0, nr)] * dg_i, 1/8)      (FP32, :178,187)
+ * dg may be NULL. */
+int viss_weights(int64_t n, const float *w, const float *bll, const int32_t *gs,
+                 const float *dcf, int nr, float *dg, float *wt, void *stream);
+
+/* w-rotation of viss_gamma_trans (vissgen3d_blockage.cu:150-151):
+ *   V_i <- V_i exp(-2 pi i w_i)  (FP64 phase), complex64 in place; w FP32. */
+int viss_wrot(int64_t n, const float *w, float *V, void *stream);
+
+/* coef_i = wt_i * V_i (complex64), optionally conj-copied: when
+ * mirror > 0, rows [mirror, 2 mirror) of V are first set to conj of rows
+ * [0, mirror) (vissgen3d_blockage.cu:100). */
+int viss_conj_mirror(int64_t mirror, float *V, void *stream);
+int viss_scale_coef(int64_t n, const float *wt, const float *V, float *coef, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VISS_H */

@@ -1,0 +1,485 @@
+// capi.cu -- the extern "C" boundary (include/viss.h) and the plan.
+//
+// The reference reports failures through CHECK (error.cuh:4-19), which prints
+// and calls exit(1).  Every entry point here returns a status instead and
+// records the message in a thread-local string (viss_last_error).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "viss.h"
+#include "viss_common.cuh"
+
+namespace viss {
+// launchers (healpix.cu, geometry.cu, visibility.cu, dcf.cu)
+cudaError_t launch_mk_pix2xy(int32_t *, int32_t *, cudaStream_t);
+cudaError_t launch_pix2ang(long long, int, long long, long long, double *, double *, double *, int,
+                           cudaStream_t);
+cudaError_t launch_pix_convert(long long, int, int, long long *, cudaStream_t);
+cudaError_t launch_sky_pre(long long, const float *, const float *, const float *, float, double *,
+                           float *, cudaStream_t);
+cudaError_t launch_occulters(long long, const double *, double, int, double, double4 *,
+                             cudaStream_t);
+cudaError_t launch_mask_bits(long long, long long, const double *, const int32_t *,
+                             const double4 *, uint32_t *, cudaStream_t);
+cudaError_t launch_stage_pixels(long long, long long, const double *, double4 *, double4 *,
+                                cudaStream_t);
+cudaError_t launch_stage_sky(long long, long long, const double4 *, const float *, float,
+                             double4 *, cudaStream_t);
+cudaError_t launch_stage_coef(long long, long long, const float2 *, float2 *, cudaStream_t);
+cudaError_t launch_stage_samples(long long, const double *, const double *, const int32_t *,
+                                 double4 *, int4 *, unsigned long long *, cudaStream_t);
+cudaError_t launch_dcf(long long, const float *, int, int, int32_t *, unsigned int *, float *,
+                       int, cudaStream_t);
+cudaError_t launch_weights(long long, const float *, const float *, const int32_t *,
+                           const float *, int, float *, float *, cudaStream_t);
+cudaError_t launch_wrot(long long, const float *, float2 *, cudaStream_t);
+cudaError_t launch_conj_mirror(long long, float2 *, cudaStream_t);
+cudaError_t launch_scale_coef(long long, const float *, const float2 *, float2 *, cudaStream_t);
+}  // namespace viss
+
+#include "visibility.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string &msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return VISS_ERR_CUDA;
+}
+
+#define VISS_CUDA(call, where)                       \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+  } while (0)
+
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+  return n > 0 ? n : 148;
+}
+
+template <class T>
+int ensure(T *&ptr, size_t &cap, size_t bytes, const char *what) {
+  if (bytes <= cap && ptr) return VISS_OK;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(VISS_ERR_ALLOC, std::string("cudaMalloc failed for ") + what + " (" +
+                                    std::to_string(bytes) + " bytes)");
+  }
+  ptr = static_cast<T *>(p);
+  cap = bytes;
+  return VISS_OK;
+}
+
+}  // namespace
+
+struct viss_plan {
+  int device = 0;
+  int nsm = 148;
+  // pixels
+  long long J = 0, Jpad = 0;
+  int ntiles = 0;
+  double4 *pix = nullptr;    size_t pix_cap = 0;
+  double4 *pixsky = nullptr; size_t pixsky_cap = 0;
+  double4 *cones = nullptr;  size_t cones_cap = 0;
+  // samples
+  long long K = 0, Kpad = 0;
+  double4 *samp = nullptr; size_t samp_cap = 0;
+  int4 *refs = nullptr;    size_t refs_cap = 0;
+  bool has_refs = false;
+  double4 *occ = nullptr;  size_t occ_cap = 0;
+  long long G = 0;
+  float2 *coef = nullptr;  size_t coef_cap = 0;
+  double max_turns = 0;
+  // workspace + device status words
+  void *part = nullptr;    size_t part_cap = 0;
+  unsigned long long *dev_words = nullptr;  // [0] evaluated counter, [1] error flags, [2] bound
+  size_t dev_words_cap = 0;
+  long long last_total = 0;
+  cudaStream_t last_stream = nullptr;
+  // launch shape
+  int fwd_R = 4;
+  int fwd_waves = 16;
+  int adj_waves = 16;
+};
+
+namespace {
+
+int fwd_chunks(const viss_plan *p, int R, bool fp64) {
+  const long long per = viss::forward_samples_per_block(R, fp64);
+  const long long blocks = (p->K + per - 1) / per;
+  const long long slots = static_cast<long long>(p->nsm) * (fp64 ? 1 : 2);
+  long long c = (static_cast<long long>(p->fwd_waves) * slots + blocks - 1) / blocks;
+  c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 2)));
+  return static_cast<int>(c);
+}
+
+int adj_chunks(const viss_plan *p, bool fp64, int *samples_per_chunk) {
+  const long long per = 8LL * viss::kTilePix;  // pixels per CTA
+  const long long blocks = (p->Jpad + per - 1) / per;
+  const long long slots = static_cast<long long>(p->nsm) * (fp64 ? 1 : 2);
+  long long c = (static_cast<long long>(p->adj_waves) * slots + blocks - 1) / blocks;
+  const long long max_c = std::max<long long>(1, (p->K + 255) / 256);
+  c = std::max<long long>(1, std::min(c, max_c));
+  long long spc = (p->K + c - 1) / c;
+  spc = (spc + viss::kSampTile - 1) / viss::kSampTile * viss::kSampTile;
+  c = (p->K + spc - 1) / spc;
+  *samples_per_chunk = static_cast<int>(spc);
+  return static_cast<int>(std::max<long long>(1, c));
+}
+
+cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+int viss_version(void) { return 1; }
+
+const char *viss_status_string(int status) {
+  switch (status) {
+    case VISS_OK: return "ok";
+    case VISS_ERR_ARG: return "invalid argument";
+    case VISS_ERR_CUDA: return "CUDA runtime error";
+    case VISS_ERR_ALLOC: return "device allocation failed";
+    case VISS_ERR_TIMEOUT: return "bounded device wait gave up";
+    case VISS_ERR_NOTFINITE: return "non-finite input";
+    case VISS_ERR_IO: return "file missing or malformed";
+    case VISS_ERR_STATE: return "plan state incomplete";
+    default: return "unknown status";
+  }
+}
+
+size_t viss_last_error(char *buf, size_t len) {
+  if (buf && len) {
+    const size_t n = std::min(len - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), n);
+    buf[n] = '\0';
+  }
+  return g_last_error.size();
+}
+
+// ----------------------------------------------------------------- HEALPix
+int viss_mk_pix2xy(int32_t *pix2x, int32_t *pix2y, void *stream) {
+  if (!pix2x || !pix2y) return fail(VISS_ERR_ARG, "viss_mk_pix2xy: null output");
+  VISS_CUDA(viss::launch_mk_pix2xy(pix2x, pix2y, as_stream(stream)), "viss_mk_pix2xy");
+  return VISS_OK;
+}
+
+static int check_nside(int nside, const char *who) {
+  if (nside < 1 || nside > (1 << 13))
+    return fail(VISS_ERR_ARG, std::string(who) + ": nside must be in [1, 8192]");
+  return VISS_OK;
+}
+
+int viss_pix2ang(int nside, int scheme, int64_t first, int64_t count, double *theta, double *phi,
+                 double *xyz, void *stream) {
+  if (int s = check_nside(nside, "viss_pix2ang")) return s;
+  const long long npix = 12LL * nside * nside;
+  if (scheme != VISS_RING && scheme != VISS_NESTED)
+    return fail(VISS_ERR_ARG, "viss_pix2ang: scheme must be VISS_RING or VISS_NESTED");
+  if (first < 0 || count < 0 || first + count > npix)
+    return fail(VISS_ERR_ARG, "viss_pix2ang: pixel range outside [0, 12 nside^2)");
+  VISS_CUDA(viss::launch_pix2ang(nside, scheme, first, count, theta, phi, xyz, 0, as_stream(stream)),
+            "viss_pix2ang");
+  return VISS_OK;
+}
+
+int viss_pix_convert(int nside, int from_scheme, int to_scheme, int64_t *out, void *stream) {
+  if (int s = check_nside(nside, "viss_pix_convert")) return s;
+  if (!out) return fail(VISS_ERR_ARG, "viss_pix_convert: null output");
+  if ((from_scheme != 0 && from_scheme != 1) || (to_scheme != 0 && to_scheme != 1))
+    return fail(VISS_ERR_ARG, "viss_pix_convert: bad scheme");
+  VISS_CUDA(viss::launch_pix_convert(nside, from_scheme, to_scheme,
+                                     reinterpret_cast<long long *>(out), as_stream(stream)),
+            "viss_pix_convert");
+  return VISS_OK;
+}
+
+int viss_pix2lmn(int nside, int scheme, double *lmn, void *stream) {
+  if (int s = check_nside(nside, "viss_pix2lmn")) return s;
+  if (!lmn) return fail(VISS_ERR_ARG, "viss_pix2lmn: null output");
+  if (scheme != VISS_RING && scheme != VISS_NESTED) return fail(VISS_ERR_ARG, "viss_pix2lmn: bad scheme");
+  const long long npix = 12LL * nside * nside;
+  VISS_CUDA(viss::launch_pix2ang(nside, scheme, 0, npix, nullptr, nullptr, lmn, 1, as_stream(stream)),
+            "viss_pix2lmn");
+  return VISS_OK;
+}
+
+int viss_sky_pre(int64_t npix, const float *theta, const float *phi, const float *B, float s,
+                 double *lmn, float *B_out, void *stream) {
+  if (npix < 0 || !theta || !phi || !lmn || (B_out && !B))
+    return fail(VISS_ERR_ARG, "viss_sky_pre: bad arguments");
+  VISS_CUDA(viss::launch_sky_pre(npix, theta, phi, B, s, lmn, B_out, as_stream(stream)),
+            "viss_sky_pre");
+  return VISS_OK;
+}
+
+// --------------------------------------------------------------- occulters
+double viss_cone_threshold(float R, float h) {
+  // vissgen3d_blockage.cu:251-252, on the host in FP32 like the reference.
+  const float th = asinf(R / (R + h));
+  const float ph = static_cast<float>(M_PI - static_cast<double>(th));
+  return std::cos(static_cast<double>(ph));
+}
+
+int viss_occulters(int64_t n, const double *P, double R, int mode, double fixed_thr, double *occ,
+                   void *stream) {
+  if (n < 0 || (n > 0 && (!P || !occ)) || (mode != 0 && mode != 1))
+    return fail(VISS_ERR_ARG, "viss_occulters: bad arguments");
+  if (mode == 0 && !(R > 0)) return fail(VISS_ERR_ARG, "viss_occulters: R must be > 0");
+  if (reinterpret_cast<uintptr_t>(occ) % 16)
+    return fail(VISS_ERR_ARG, "viss_occulters: occ must be 16-byte aligned");
+  VISS_CUDA(viss::launch_occulters(n, P, R, mode, fixed_thr, reinterpret_cast<double4 *>(occ),
+                                   as_stream(stream)),
+            "viss_occulters");
+  return VISS_OK;
+}
+
+int viss_mask_bits(int64_t K, int64_t J, const double *lmn, const int32_t *refs, const double *occ,
+                   uint32_t *bits, void *stream) {
+  if (K < 0 || J < 0 || (K > 0 && J > 0 && (!lmn || !refs || !occ || !bits)))
+    return fail(VISS_ERR_ARG, "viss_mask_bits: bad arguments");
+  if (reinterpret_cast<uintptr_t>(occ) % 16)
+    return fail(VISS_ERR_ARG, "viss_mask_bits: occ must be 16-byte aligned");
+  VISS_CUDA(viss::launch_mask_bits(K, J, lmn, refs, reinterpret_cast<const double4 *>(occ), bits,
+                                   as_stream(stream)),
+            "viss_mask_bits");
+  return VISS_OK;
+}
+
+// ------------------------------------------------------------------- plans
+int viss_plan_create(viss_plan **plan) {
+  if (!plan) return fail(VISS_ERR_ARG, "viss_plan_create: null plan");
+  viss_plan *p = new (std::nothrow) viss_plan();
+  if (!p) return fail(VISS_ERR_ALLOC, "viss_plan_create: out of host memory");
+  VISS_CUDA(cudaGetDevice(&p->device), "viss_plan_create");
+  p->nsm = sm_count();
+  if (int s = ensure(p->dev_words, p->dev_words_cap, 4 * sizeof(unsigned long long), "status words")) {
+    delete p;
+    return s;
+  }
+  cudaMemset(p->dev_words, 0, 4 * sizeof(unsigned long long));
+  *plan = p;
+  return VISS_OK;
+}
+
+int viss_plan_destroy(viss_plan *p) {
+  if (!p) return VISS_OK;
+  void *bufs[] = {p->pix, p->pixsky, p->cones, p->samp, p->refs, p->occ, p->coef, p->part, p->dev_words};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  delete p;
+  return VISS_OK;
+}
+
+int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *stream) {
+  if (!p || J <= 0 || !lmn) return fail(VISS_ERR_ARG, "viss_plan_set_pixels: bad arguments");
+  if (J > (1LL << 31) * viss::kTilePix / 2)
+    return fail(VISS_ERR_ARG, "viss_plan_set_pixels: too many pixels");
+  const long long Jpad = (J + viss::kTilePix - 1) / viss::kTilePix * viss::kTilePix;
+  const long long nt = Jpad / viss::kTilePix;
+  if (int s = ensure(p->pix, p->pix_cap, sizeof(double4) * Jpad, "pixel records")) return s;
+  if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * Jpad, "pixel+sky records")) return s;
+  if (int s = ensure(p->cones, p->cones_cap, sizeof(double4) * nt, "tile cones")) return s;
+  VISS_CUDA(viss::launch_stage_pixels(J, Jpad, lmn, p->pix, p->cones, as_stream(stream)),
+            "viss_plan_set_pixels");
+  p->J = J;
+  p->Jpad = Jpad;
+  p->ntiles = static_cast<int>(nt);
+  return VISS_OK;
+}
+
+int viss_plan_set_samples(viss_plan *p, int64_t K, const double *uvw, const double *off,
+                          const int32_t *refs, int64_t G, const double *occ, void *stream) {
+  if (!p || K <= 0 || !uvw) return fail(VISS_ERR_ARG, "viss_plan_set_samples: bad arguments");
+  if (refs && (G <= 0 || !occ))
+    return fail(VISS_ERR_ARG, "viss_plan_set_samples: refs given without an occulter table");
+  if (K > (1LL << 40)) return fail(VISS_ERR_ARG, "viss_plan_set_samples: too many samples");
+  const cudaStream_t st = as_stream(stream);
+  const long long Kpad = (K + 1) & ~1LL;
+  if (int s = ensure(p->samp, p->samp_cap, sizeof(double4) * Kpad, "sample records")) return s;
+  if (int s = ensure(p->coef, p->coef_cap, sizeof(float2) * Kpad, "coefficients")) return s;
+  if (refs) {
+    if (int s = ensure(p->refs, p->refs_cap, sizeof(int4) * Kpad, "occulter refs")) return s;
+    if (int s = ensure(p->occ, p->occ_cap, sizeof(double4) * G, "occulter table")) return s;
+    VISS_CUDA(cudaMemcpyAsync(p->occ, occ, sizeof(double4) * G, cudaMemcpyDeviceToDevice, st),
+              "viss_plan_set_samples: occulters");
+  }
+  VISS_CUDA(cudaMemsetAsync(p->dev_words + 2, 0, sizeof(unsigned long long), st),
+            "viss_plan_set_samples");
+  VISS_CUDA(viss::launch_stage_samples(K, uvw, off, refs, p->samp, refs ? p->refs : nullptr,
+                                       p->dev_words + 2, st),
+            "viss_plan_set_samples");
+  unsigned long long bits = 0;
+  VISS_CUDA(cudaMemcpyAsync(&bits, p->dev_words + 2, sizeof(bits), cudaMemcpyDeviceToHost, st),
+            "viss_plan_set_samples: bound");
+  VISS_CUDA(cudaStreamSynchronize(st), "viss_plan_set_samples: sync");
+  double bound;
+  std::memcpy(&bound, &bits, sizeof(bound));
+  if (!std::isfinite(bound))
+    return fail(VISS_ERR_NOTFINITE, "viss_plan_set_samples: non-finite uvw or offset");
+  p->K = K;
+  p->Kpad = Kpad;
+  p->has_refs = refs != nullptr;
+  p->G = refs ? G : 0;
+  p->max_turns = bound;
+  return VISS_OK;
+}
+
+static int workspace(viss_plan *p, size_t bytes) {
+  return ensure(p->part, p->part_cap, bytes, "partial-sum workspace");
+}
+
+int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stream) {
+  if (!p || !sky || !V) return fail(VISS_ERR_ARG, "viss_forward: bad arguments");
+  if (p->J <= 0 || p->K <= 0) return fail(VISS_ERR_STATE, "viss_forward: pixels or samples not set");
+  const bool fp64 = (flags & VISS_FP64) != 0;
+  const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
+  if (!fp64 && !(p->max_turns < viss::kMaxTurns))
+    return fail(VISS_ERR_ARG, "viss_forward: |u|+|v|+|w|+|off| exceeds 2^28 turns; use VISS_FP64");
+  const cudaStream_t st = as_stream(stream);
+  const int R = fp64 ? 2 : p->fwd_R;
+  const int nchunk = fwd_chunks(p, R, fp64);
+  if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * p->K)) return s;
+  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, sky, 1.0f, p->pixsky, st), "viss_forward: sky");
+  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 2 * sizeof(unsigned long long), st), "viss_forward");
+  viss::FwdParams fp;
+  fp.samp = p->samp;
+  fp.refs = masked ? p->refs : nullptr;
+  fp.occ = masked ? p->occ : nullptr;
+  fp.pix = p->pixsky;
+  fp.cones = p->cones;
+  fp.K = p->K;
+  fp.ntiles = p->ntiles;
+  fp.tiles_per_chunk = (p->ntiles + nchunk - 1) / nchunk;
+  const int real_chunks = (p->ntiles + fp.tiles_per_chunk - 1) / fp.tiles_per_chunk;
+  fp.part = static_cast<double2 *>(p->part);
+  fp.counter = p->dev_words;
+  fp.err = reinterpret_cast<int *>(p->dev_words + 1);
+  fp.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
+  VISS_CUDA(viss::launch_forward(fp, R, real_chunks, masked, fp64, st), "viss_forward: kernel");
+  VISS_CUDA(viss::launch_reduce_fwd(p->K, real_chunks, fp.part, reinterpret_cast<float2 *>(V),
+                                    (flags & VISS_ACCUMULATE) ? 1 : 0, st),
+            "viss_forward: reduce");
+  p->last_total = p->K * p->J;
+  p->last_stream = st;
+  return VISS_OK;
+}
+
+int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int flags, void *stream) {
+  if (!p || !coef || !image) return fail(VISS_ERR_ARG, "viss_adjoint: bad arguments");
+  if (p->J <= 0 || p->K <= 0) return fail(VISS_ERR_STATE, "viss_adjoint: pixels or samples not set");
+  const bool fp64 = (flags & VISS_FP64) != 0;
+  const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
+  if (!fp64 && !(p->max_turns < viss::kMaxTurns))
+    return fail(VISS_ERR_ARG, "viss_adjoint: |u|+|v|+|w|+|off| exceeds 2^28 turns; use VISS_FP64");
+  const cudaStream_t st = as_stream(stream);
+  int spc = 0;
+  const int nchunk = adj_chunks(p, fp64, &spc);
+  if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->Jpad)) return s;
+  VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
+            "viss_adjoint: coef");
+  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 2 * sizeof(unsigned long long), st), "viss_adjoint");
+  viss::AdjParams ap;
+  ap.samp = p->samp;
+  ap.coef = p->coef;
+  ap.refs = masked ? p->refs : nullptr;
+  ap.occ = masked ? p->occ : nullptr;
+  ap.pix = p->pix;
+  ap.cones = p->cones;
+  ap.K = p->K;
+  ap.Jpad = p->Jpad;
+  ap.samples_per_chunk = spc;
+  ap.part = static_cast<double *>(p->part);
+  ap.counter = p->dev_words;
+  ap.err = reinterpret_cast<int *>(p->dev_words + 1);
+  ap.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
+  VISS_CUDA(viss::launch_adjoint(ap, nchunk, masked, fp64, st), "viss_adjoint: kernel");
+  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, ap.part, scale, image,
+                                    (flags & VISS_ACCUMULATE) ? 1 : 0, st),
+            "viss_adjoint: reduce");
+  p->last_total = p->K * p->J;
+  p->last_stream = st;
+  return VISS_OK;
+}
+
+int viss_plan_last_counts(viss_plan *p, int64_t *evaluated, int64_t *total) {
+  if (!p) return fail(VISS_ERR_ARG, "viss_plan_last_counts: null plan");
+  unsigned long long w[2] = {0, 0};
+  VISS_CUDA(cudaStreamSynchronize(p->last_stream), "viss_plan_last_counts: sync");
+  VISS_CUDA(cudaMemcpy(w, p->dev_words, sizeof(w), cudaMemcpyDeviceToHost), "viss_plan_last_counts");
+  if (evaluated) *evaluated = static_cast<int64_t>(w[0]);
+  if (total) *total = p->last_total;
+  if (w[1] & viss::kErrTimeout)
+    return fail(VISS_ERR_TIMEOUT, "a bounded shared-memory staging wait gave up in the last kernel");
+  return VISS_OK;
+}
+
+// --------------------------------------------------------------------- DCF
+int viss_dcf(int64_t n, const float *bll, int nr, int multiplicity, int32_t *gs, uint32_t *counts,
+             float *dcf, void *stream) {
+  if (n < 0 || nr < 1 || nr > (1 << 17) || !dcf || (n > 0 && !bll) || multiplicity < 1)
+    return fail(VISS_ERR_ARG, "viss_dcf: bad arguments (nr must be in [1, 131072])");
+  const cudaStream_t st = as_stream(stream);
+  unsigned int *cnt = counts;
+  unsigned int *tmp = nullptr;
+  if (!cnt) {
+    VISS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(unsigned int) * nr, st),
+              "viss_dcf: counts");
+    cnt = tmp;
+  }
+  cudaError_t e = viss::launch_dcf(n, bll, nr, multiplicity, gs, cnt, dcf, sm_count(), st);
+  if (tmp) cudaFreeAsync(tmp, st);
+  if (e != cudaSuccess) return cuda_fail(e, "viss_dcf");
+  return VISS_OK;
+}
+
+int viss_weights(int64_t n, const float *w, const float *bll, const int32_t *gs, const float *dcf,
+                 int nr, float *dg, float *wt, void *stream) {
+  if (n < 0 || (n > 0 && (!w || !bll)) || (wt && (!gs || !dcf)) || nr < 0)
+    return fail(VISS_ERR_ARG, "viss_weights: bad arguments");
+  VISS_CUDA(viss::launch_weights(n, w, bll, gs, dcf, nr, dg, wt, as_stream(stream)), "viss_weights");
+  return VISS_OK;
+}
+
+int viss_wrot(int64_t n, const float *w, float *V, void *stream) {
+  if (n < 0 || (n > 0 && (!w || !V))) return fail(VISS_ERR_ARG, "viss_wrot: bad arguments");
+  VISS_CUDA(viss::launch_wrot(n, w, reinterpret_cast<float2 *>(V), as_stream(stream)), "viss_wrot");
+  return VISS_OK;
+}
+
+int viss_conj_mirror(int64_t mirror, float *V, void *stream) {
+  if (mirror < 0 || (mirror > 0 && !V)) return fail(VISS_ERR_ARG, "viss_conj_mirror: bad arguments");
+  VISS_CUDA(viss::launch_conj_mirror(mirror, reinterpret_cast<float2 *>(V), as_stream(stream)),
+            "viss_conj_mirror");
+  return VISS_OK;
+}
+
+int viss_scale_coef(int64_t n, const float *wt, const float *V, float *coef, void *stream) {
+  if (n < 0 || (n > 0 && (!wt || !V || !coef))) return fail(VISS_ERR_ARG, "viss_scale_coef: bad arguments");
+  VISS_CUDA(viss::launch_scale_coef(n, wt, reinterpret_cast<const float2 *>(V),
+                                    reinterpret_cast<float2 *>(coef), as_stream(stream)),
+            "viss_scale_coef");
+  return VISS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,203 @@
+// geometry.cu -- occulter tables, mask bits, staging layouts and tile cones.
+//
+// The occultation predicate of the reference (vissgen3d_blockage.cu:88-94 in
+// the forward kernel, :180-186 in the imaging kernel) is
+//   acosf(s.P / |P|) <= phi,   phi = pi - asinf(R/(R+h))   (:249-252)
+// per (sample, pixel), for both satellites of the baseline.  Here it is the
+// acos-free equivalent dot(s, P/|P|) >= cos(phi), evaluated in FP64 with a
+// fixed operation order (dot_exact) so that the CPU oracle reproduces every
+// bit; the same form with thr = -sqrt(1 - (R/|P|)^2) is the exact ray-sphere
+// test, and with q = -e, thr = -cos(rho) an Earth cap of radius rho.
+#include "viss_common.cuh"
+
+namespace viss {
+
+__global__ void k_occulters(long long n, const double *P, double R, int mode, double fixed_thr,
+                            double4 *occ) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = P[3 * i], y = P[3 * i + 1], z = P[3 * i + 2];
+  const double r = __dsqrt_rn(__fma_rn(z, z, __fma_rn(y, y, __dmul_rn(x, x))));
+  double4 o;
+  o.x = __ddiv_rn(x, r);
+  o.y = __ddiv_rn(y, r);
+  o.z = __ddiv_rn(z, r);
+  if (mode == 0) {
+    const double rho = __ddiv_rn(R, r);
+    o.w = -__dsqrt_rn(__dadd_rn(1.0, -__dmul_rn(rho, rho)));
+  } else {
+    o.w = fixed_thr;
+  }
+  occ[i] = o;
+}
+
+__device__ __forceinline__ bool visible3(const int32_t *r, const double4 *occ, double s0,
+                                         double s1, double s2) {
+  for (int c = 0; c < 3; ++c) {
+    const int g = r[c];
+    if (g < 0) continue;
+    const double4 q = occ[g];
+    if (!(dot_exact(s0, s1, s2, q) >= q.w)) return false;
+  }
+  return true;
+}
+
+// One warp per (sample row, 32-pixel word).
+__global__ void k_mask_bits(long long K, long long J, const double *lmn, const int32_t *refs,
+                            const double4 *occ, uint32_t *bits) {
+  const long long W = (J + 31) / 32;
+  const long long word = static_cast<long long>(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (word >= K * W) return;
+  const long long k = word / W, jw = word - k * W;
+  const long long j = jw * 32 + lane;
+  bool v = false;
+  if (j < J) v = visible3(refs + 3 * k, occ, lmn[3 * j], lmn[3 * j + 1], lmn[3 * j + 2]);
+  const uint32_t b = __ballot_sync(0xffffffffu, v);
+  if (lane == 0) bits[word] = b;
+}
+
+// Pixel staging: lmn (J x 3) -> double4 records, padded to Jpad with copies
+// of the last pixel (they never reach an output: sky is zero there and the
+// adjoint drops them).
+__global__ void k_stage_pixels(long long J, long long Jpad, const double *lmn, double4 *pix) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= Jpad) return;
+  const long long s = i < J ? i : J - 1;
+  pix[i] = make_double4(lmn[3 * s], lmn[3 * s + 1], lmn[3 * s + 2], 0.0);
+}
+
+// Bounding cone of each kTilePix-pixel tile: centre = normalised mean,
+// radius = max chord |s - c| plus a relative margin.  One warp per tile.
+__global__ void k_tile_cones(long long ntiles, const double4 *pix, double4 *cones) {
+  const long long t = static_cast<long long>(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (t >= ntiles) return;
+  double sx = 0, sy = 0, sz = 0;
+  for (int p = lane; p < kTilePix; p += 32) {
+    const double4 q = pix[t * kTilePix + p];
+    sx += q.x; sy += q.y; sz += q.z;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+  }
+  const double nrm = sqrt(sx * sx + sy * sy + sz * sz);
+  double cx = 1, cy = 0, cz = 0;
+  if (nrm > 1e-6) { cx = sx / nrm; cy = sy / nrm; cz = sz / nrm; }
+  double rho = 0;
+  for (int p = lane; p < kTilePix; p += 32) {
+    const double4 q = pix[t * kTilePix + p];
+    const double dx = q.x - cx, dy = q.y - cy, dz = q.z - cz;
+    rho = fmax(rho, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  for (int o = 16; o > 0; o >>= 1) rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+  if (lane == 0) {
+    if (nrm <= 1e-6) rho = 4.0;  // degenerate tile: always "test every pixel"
+    cones[t] = make_double4(cx, cy, cz, rho * (1.0 + 1e-9) + 1e-12);
+  }
+}
+
+// Sky staging: pixel record + sky value in the low word of .w (zero past J),
+// so one 32-byte record per pixel carries everything the forward reads.
+__global__ void k_stage_sky(long long J, long long Jpad, const double4 *pix, const float *sky,
+                            float scale, double4 *out) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= Jpad) return;
+  double4 r = pix[i];
+  const float v = i < J ? __fmul_rn(sky[i], scale) : 0.0f;
+  r.w = __hiloint2double(0, __float_as_int(v));
+  out[i] = r;
+}
+
+// Sample staging: uvw (K x 3), off (K or null), refs (K x 3 or null).
+__global__ void k_stage_samples(long long K, const double *uvw, const double *off,
+                                const int32_t *refs, double4 *samp, int4 *ref4) {
+  const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  samp[k] = make_double4(uvw[3 * k], uvw[3 * k + 1], uvw[3 * k + 2], off ? off[k] : 0.0);
+  if (ref4) {
+    if (refs) ref4[k] = make_int4(refs[3 * k], refs[3 * k + 1], refs[3 * k + 2], -1);
+    else ref4[k] = make_int4(-1, -1, -1, -1);
+  }
+}
+
+// |u.s + off| bound check for the split path: max over samples of
+// |u|+|v|+|w|+|off| (>= |u.s + off| for unit s).  Non-finite -> +inf.
+__global__ void k_sample_bound(long long K, const double4 *samp, unsigned long long *out) {
+  const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  double b = 0;
+  if (k < K) {
+    const double4 s = samp[k];
+    b = fabs(s.x) + fabs(s.y) + fabs(s.z) + fabs(s.w);
+    if (!(b <= 1e300)) b = __longlong_as_double(0x7ff0000000000000ll);
+  }
+  for (int o = 16; o > 0; o >>= 1) b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(b)));
+}
+
+}  // namespace viss
+
+namespace viss {
+
+static inline unsigned nblk(long long n, int bs) { return static_cast<unsigned>((n + bs - 1) / bs); }
+
+cudaError_t launch_occulters(long long n, const double *P, double R, int mode, double thr,
+                             double4 *occ, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_occulters<<<nblk(n, 256), 256, 0, st>>>(n, P, R, mode, thr, occ);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mask_bits(long long K, long long J, const double *lmn, const int32_t *refs,
+                             const double4 *occ, uint32_t *bits, cudaStream_t st) {
+  const long long words = K * ((J + 31) / 32);
+  if (words <= 0) return cudaSuccess;
+  k_mask_bits<<<nblk(words, 8), 256, 0, st>>>(K, J, lmn, refs, occ, bits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, double4 *pix,
+                                double4 *cones, cudaStream_t st) {
+  k_stage_pixels<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, lmn, pix);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long nt = Jpad / kTilePix;
+  k_tile_cones<<<nblk(nt, 8), 256, 0, st>>>(nt, pix, cones);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_sky(long long J, long long Jpad, const double4 *pix, const float *sky,
+                             float scale, double4 *out, cudaStream_t st) {
+  k_stage_sky<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, pix, sky, scale, out);
+  return cudaGetLastError();
+}
+
+// Coefficient staging for the adjoint: a 16-byte aligned copy padded to an
+// even count (bulk copies move whole 16-byte units).
+__global__ void k_stage_coef(long long K, long long Kpad, const float2 *coef, float2 *out) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= Kpad) return;
+  out[i] = i < K ? coef[i] : make_float2(0.f, 0.f);
+}
+
+cudaError_t launch_stage_coef(long long K, long long Kpad, const float2 *coef, float2 *out,
+                              cudaStream_t st) {
+  if (Kpad <= 0) return cudaSuccess;
+  k_stage_coef<<<nblk(Kpad, 256), 256, 0, st>>>(K, Kpad, coef, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_samples(long long K, const double *uvw, const double *off,
+                                 const int32_t *refs, double4 *samp, int4 *ref4,
+                                 unsigned long long *bound, cudaStream_t st) {
+  if (K <= 0) return cudaSuccess;
+  k_stage_samples<<<nblk(K, 256), 256, 0, st>>>(K, uvw, off, refs, samp, ref4);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !bound) return e;
+  k_sample_bound<<<nblk(K, 256), 256, 0, st>>>(K, samp, bound);
+  return cudaGetLastError();
+}
+
+}  // namespace viss

@@ -1,0 +1,490 @@
+// visibility.cu -- the two O(K x J) kernels of the hot path.
+//
+//   forward  V_k = sum_j I_j vis_kj exp(-2 pi i (u_k.s_j + off_k))
+//            replaces healpix_moonback_viss (vissgen3d_blockage.cu:76-102)
+//   adjoint  C_j = sum_k Re(a_k exp(+2 pi i (u_k.s_j + off_k))) vis_kj
+//            replaces computeC (vissgen3d_blockage.cu:167-192)
+//
+// Both are matrix-free matvecs bound by the SFU (two MUFU ops per term:
+// sin and cos), not by HBM and not by tensor cores.  Per term the split path
+// issues: 3 DFMA (phase in FP64, already reduced to a 2^-23-turn fixed point
+// by the kMagic offset), 1 LOP3 (fraction -> float), 1 FFMA (-> radians),
+// sin/cos, 2 FFMA (accumulate).
+//
+// Work decomposition
+//   forward: a CTA owns NT*R samples (R per thread, in registers) and one
+//            chunk of pixel tiles; tiles of kTilePix pixel records stream
+//            through a 2-deep shared-memory ring filled by cp.async.bulk
+//            (TMA engine) and are read as warp-wide broadcasts.  Partial sums
+//            of each chunk go to a [chunk][K] FP64 workspace; k_reduce_fwd
+//            adds the chunks in FP64.
+//   adjoint: a warp owns one pixel tile (32 lanes x 4 pixels, in registers);
+//            a CTA owns 8 tiles and one chunk of samples, which stream through
+//            shared memory the same way.  Chunks go to a [chunk][J] FP64
+//            workspace reduced by k_reduce_adj.
+// Occultation: every tile carries a bounding cone (centre, chord radius).
+// Against a sample's occulters a tile is "all visible" (no per-term test),
+// "none visible" (skipped) or "mixed" (exact FP64 predicate per term, the
+// same operations as the CPU oracle, so the mask bits match it exactly).
+// The decision is warp-uniform: the warp votes in the forward, and in the
+// adjoint the sample is uniform across the warp.
+//
+// Accuracy: terms are summed in FP32 within a tile (<= 128 terms per
+// accumulator), tile sums are folded into a Kahan-compensated FP32 sum, and
+// chunks are added in FP64.
+#include "visibility.cuh"
+
+namespace viss {
+
+
+// Kahan-compensated add of x into (s, c).
+__device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
+  const float y = __fsub_rn(x, c);
+  const float t = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(t, s), y);
+  s = t;
+}
+
+// State of a sample (3 occulter refs) against a tile cone: min over refs of
+// cone_state (2 all visible, 0 none, 1 mixed).
+__device__ __forceinline__ int sample_state(const int4 &rf, const double4 &cone,
+                                            const double4 *occ) {
+  int st = 2;
+  if (rf.x >= 0) st = min(st, cone_state(cone, occ[rf.x]));
+  if (rf.y >= 0) st = min(st, cone_state(cone, occ[rf.y]));
+  if (rf.z >= 0) st = min(st, cone_state(cone, occ[rf.z]));
+  return st;
+}
+
+__device__ __forceinline__ bool visible_exact(const int4 &rf, const double4 *occ, double s0,
+                                              double s1, double s2) {
+  bool v = true;
+  if (rf.x >= 0) { const double4 q = occ[rf.x]; v = v && (dot_exact(s0, s1, s2, q) >= q.w); }
+  if (rf.y >= 0) { const double4 q = occ[rf.y]; v = v && (dot_exact(s0, s1, s2, q) >= q.w); }
+  if (rf.z >= 0) { const double4 q = occ[rf.z]; v = v && (dot_exact(s0, s1, s2, q) >= q.w); }
+  return v;
+}
+
+__device__ __forceinline__ float sky_of(const double4 &p) {
+  return __int_as_float(__double2loint(p.w));
+}
+
+// FP64 reference term: (cos, sin) of 2 pi (phase mod 1), phase in FP64.
+__device__ __forceinline__ void sincos_turns_fp64(double t, double &sn, double &cs) {
+  const double f = t - rint(t);
+  sincospi(2.0 * f, &sn, &cs);
+}
+
+// ======================================================================
+// forward
+// ======================================================================
+template <int NT, int R, bool MASKED, bool FP64>
+__global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p) {
+  __shared__ __align__(128) double4 s_pix[2][kTilePix];
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.x;
+  const long long kb = static_cast<long long>(blockIdx.x) * (NT * R);
+
+  double ux[R], uy[R], uz[R], mk[R];
+  int4 rf[R];
+  bool kval[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const long long k = kb + r * NT + tid;
+    kval[r] = k < p.K;
+    const double4 s = kval[r] ? p.samp[k] : make_double4(0, 0, 0, 0);
+    ux[r] = s.x; uy[r] = s.y; uz[r] = s.z;
+    const double off = p.use_off ? s.w : 0.0;
+    mk[r] = FP64 ? off : kMagic + off;
+    if (MASKED) rf[r] = kval[r] ? p.refs[k] : make_int4(-1, -1, -1, -1);
+  }
+
+  unsigned nval_warp = 0;  // valid samples of this warp
+#pragma unroll
+  for (int r = 0; r < R; ++r) nval_warp += __popc(__ballot_sync(0xffffffffu, kval[r]));
+
+  // accumulators: split -> Kahan FP32 (sum, comp); FP64 -> plain double
+  float ks_re[R], kc_re[R], ks_im[R], kc_im[R];
+  double d_re[R], d_im[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    ks_re[r] = kc_re[r] = ks_im[r] = kc_im[r] = 0.f;
+    d_re[r] = d_im[r] = 0.0;
+  }
+
+  const int t0 = blockIdx.y * p.tiles_per_chunk;
+  const int t1 = min(t0 + p.tiles_per_chunk, p.ntiles);
+  constexpr uint32_t kTileBytes = kTilePix * sizeof(double4);
+
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+    s_abort = 0;
+  }
+  __syncthreads();
+  if (tid == 0 && t0 < t1) {
+    mbar_expect_tx(&s_bar[0], kTileBytes);
+    bulk_g2s(s_pix[0], p.pix + static_cast<long long>(t0) * kTilePix, kTileBytes, &s_bar[0]);
+  }
+
+  unsigned long long evaluated = 0;
+  int it = 0;
+  for (int t = t0; t < t1; ++t, ++it) {
+    const int buf = it & 1;
+    const uint32_t par = (it >> 1) & 1;
+    if (tid == 0 && t + 1 < t1) {
+      mbar_expect_tx(&s_bar[buf ^ 1], kTileBytes);
+      bulk_g2s(s_pix[buf ^ 1], p.pix + static_cast<long long>(t + 1) * kTilePix, kTileBytes,
+               &s_bar[buf ^ 1]);
+    }
+    // classify the tile for this warp's samples
+    int mode = 2;
+    int st[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) st[r] = 2;
+    if (MASKED) {
+      const double4 cone = p.cones[t];
+      bool full = true, any = false;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (kval[r]) {
+          st[r] = sample_state(rf[r], cone, p.occ);
+          full = full && (st[r] == 2);
+          any = any || (st[r] != 0);
+        }
+      }
+      const bool wfull = __all_sync(0xffffffffu, full);
+      const bool wany = __any_sync(0xffffffffu, any);
+      mode = wfull ? 2 : (wany ? 1 : 0);
+    }
+    if (!mbar_wait_bounded(&s_bar[buf], par)) {
+      atomicOr(p.err, kErrTimeout);
+      s_abort = 1;
+    }
+    const double4 *tp = s_pix[buf];
+    if (mode != 0) {
+      if ((tid & 31) == 0) evaluated += static_cast<unsigned long long>(nval_warp) * kTilePix;
+      float t_re[R], t_im[R];
+      double e_re[R], e_im[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) { t_re[r] = t_im[r] = 0.f; e_re[r] = e_im[r] = 0.0; }
+      if (mode == 2) {
+#pragma unroll 2
+        for (int j = 0; j < kTilePix; ++j) {
+          const double4 q = tp[j];
+          const float I = sky_of(q);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
+            if (FP64) {
+              double sn, cs;
+              sincos_turns_fp64(t, sn, cs);
+              e_re[r] = fma(static_cast<double>(I), cs, e_re[r]);
+              e_im[r] = fma(-static_cast<double>(I), sn, e_im[r]);
+            } else {
+              float sn, cs;
+              __sincosf(turn_angle(t), &sn, &cs);
+              t_re[r] = fmaf(I, cs, t_re[r]);
+              t_im[r] = fmaf(-I, sn, t_im[r]);
+            }
+          }
+        }
+      } else {
+        for (int j = 0; j < kTilePix; ++j) {
+          const double4 q = tp[j];
+          const float I = sky_of(q);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const bool vis = st[r] == 2 || (st[r] == 1 && visible_exact(rf[r], p.occ, q.x, q.y, q.z));
+            const float Iv = vis ? I : 0.f;
+            const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
+            if (FP64) {
+              double sn, cs;
+              sincos_turns_fp64(t, sn, cs);
+              e_re[r] = fma(static_cast<double>(Iv), cs, e_re[r]);
+              e_im[r] = fma(-static_cast<double>(Iv), sn, e_im[r]);
+            } else {
+              float sn, cs;
+              __sincosf(turn_angle(t), &sn, &cs);
+              t_re[r] = fmaf(Iv, cs, t_re[r]);
+              t_im[r] = fmaf(-Iv, sn, t_im[r]);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (FP64) {
+          d_re[r] += e_re[r];
+          d_im[r] += e_im[r];
+        } else {
+          kahan_add(ks_re[r], kc_re[r], t_re[r]);
+          kahan_add(ks_im[r], kc_im[r], t_im[r]);
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with buf before it is refilled
+    if (s_abort) {
+      // a copy was lost: let the other buffer's copy (if any) land, bounded
+      if (tid == 0 && t + 1 < t1) mbar_wait_bounded(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
+      break;
+    }
+  }
+
+  if (p.counter && (tid & 31) == 0 && evaluated) atomicAdd(p.counter, evaluated);
+  double2 *out = p.part + static_cast<long long>(blockIdx.y) * p.K;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const long long k = kb + r * NT + tid;
+    if (!kval[r]) continue;
+    double2 v;
+    if (FP64) {
+      v.x = d_re[r];
+      v.y = d_im[r];
+    } else {
+      v.x = static_cast<double>(ks_re[r]) - static_cast<double>(kc_re[r]);
+      v.y = static_cast<double>(ks_im[r]) - static_cast<double>(kc_im[r]);
+    }
+    out[k] = v;
+  }
+}
+
+// V_k = sum over chunks (FP64) -> complex64, optionally accumulated.
+__global__ void k_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V,
+                             int accumulate) {
+  const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  double re = 0, im = 0;
+  for (int c = 0; c < nchunk; ++c) {
+    const double2 v = part[static_cast<long long>(c) * K + k];
+    re += v.x;
+    im += v.y;
+  }
+  if (accumulate) {
+    const float2 o = V[k];
+    re += o.x;
+    im += o.y;
+  }
+  V[k] = make_float2(static_cast<float>(re), static_cast<float>(im));
+}
+
+// ======================================================================
+// adjoint
+// ======================================================================
+template <int NT, int P, bool MASKED, bool FP64>
+__global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p) {
+  static_assert(P * 32 == kTilePix, "one warp covers one pixel tile");
+  __shared__ __align__(128) double4 s_samp[2][kSampTile];
+  __shared__ __align__(16) float2 s_coef[2][kSampTile];
+  __shared__ __align__(16) int4 s_refs[MASKED ? 2 : 1][MASKED ? kSampTile : 1];
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kWarps = NT / 32;
+  const long long tile = static_cast<long long>(blockIdx.x) * kWarps + warp;  // pixel tile of this warp
+  const long long pbase = tile * kTilePix;
+  const bool tile_ok = pbase < p.Jpad;
+
+  double sx[P], sy[P], sz[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const long long j = pbase + q * 32 + lane;
+    const double4 v = tile_ok ? p.pix[j] : make_double4(0, 0, 1, 0);
+    sx[q] = v.x; sy[q] = v.y; sz[q] = v.z;
+  }
+  const double4 cone = (MASKED && tile_ok) ? p.cones[tile] : make_double4(0, 0, 1, 4.0);
+
+  float ks[P], kc[P];
+  double dacc[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) { ks[q] = kc[q] = 0.f; dacc[q] = 0.0; }
+
+  const long long k0 = static_cast<long long>(blockIdx.y) * p.samples_per_chunk;
+  const long long k1 = min(k0 + p.samples_per_chunk, p.K);
+  const int ntile = static_cast<int>((k1 - k0 + kSampTile - 1) / kSampTile);
+
+  auto issue = [&](int it, int buf) {
+    const long long kk = k0 + static_cast<long long>(it) * kSampTile;
+    const int n = static_cast<int>(min(static_cast<long long>(kSampTile), k1 - kk));
+    // sizes in multiples of 16 B: samp 32 B each, coef 8 B each (pad to even), refs 16 B
+    const int nc = (n + 1) & ~1;
+    uint32_t bytes = n * 32u + nc * 8u + (MASKED ? n * 16u : 0u);
+    mbar_expect_tx(&s_bar[buf], bytes);
+    bulk_g2s(s_samp[buf], p.samp + kk, n * 32u, &s_bar[buf]);
+    bulk_g2s(s_coef[buf], p.coef + kk, nc * 8u, &s_bar[buf]);
+    if (MASKED) bulk_g2s(s_refs[buf], p.refs + kk, n * 16u, &s_bar[buf]);
+  };
+
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+    s_abort = 0;
+  }
+  __syncthreads();
+  if (tid == 0 && ntile > 0) issue(0, 0);
+
+  unsigned long long evaluated = 0;
+  for (int it = 0; it < ntile; ++it) {
+    const int buf = it & 1;
+    const uint32_t par = (it >> 1) & 1;
+    if (tid == 0 && it + 1 < ntile) issue(it + 1, buf ^ 1);
+    if (!mbar_wait_bounded(&s_bar[buf], par)) {
+      atomicOr(p.err, kErrTimeout);
+      s_abort = 1;
+    }
+    const long long kk = k0 + static_cast<long long>(it) * kSampTile;
+    const int n = static_cast<int>(min(static_cast<long long>(kSampTile), k1 - kk));
+    const double4 *sp = s_samp[buf];
+    const float2 *cp = s_coef[buf];
+    for (int g = 0; g < n; g += 32) {
+      // lane l classifies sample g+l against this warp's tile
+      int st = 2;
+      if (MASKED) {
+        st = 0;
+        if (g + lane < n && tile_ok) st = sample_state(s_refs[buf][g + lane], cone, p.occ);
+      }
+      const int gn = min(32, n - g);
+      unsigned long long ev = 0;
+      float t_acc[P];
+      double e_acc[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) { t_acc[q] = 0.f; e_acc[q] = 0.0; }
+      for (int i = 0; i < gn; ++i) {
+        const int sst = MASKED ? __shfl_sync(0xffffffffu, st, i) : 2;
+        if (sst == 0) continue;
+        ev += kTilePix;
+        const double4 u = sp[g + i];
+        const float2 a = cp[g + i];
+        const double uoff = p.use_off ? u.w : 0.0;
+        const double m = FP64 ? uoff : kMagic + uoff;
+        int4 rfi;
+        if (MASKED && sst == 1) rfi = s_refs[buf][g + i];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          bool vis = true;
+          if (MASKED && sst == 1) vis = visible_exact(rfi, p.occ, sx[q], sy[q], sz[q]);
+          const double t = fma(u.z, sz[q], fma(u.y, sy[q], fma(u.x, sx[q], m)));
+          if (FP64) {
+            double sn, cs;
+            sincos_turns_fp64(t, sn, cs);
+            const double c = fma(static_cast<double>(a.x), cs, -static_cast<double>(a.y) * sn);
+            e_acc[q] += vis ? c : 0.0;
+          } else {
+            float sn, cs;
+            __sincosf(turn_angle(t), &sn, &cs);
+            const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
+            t_acc[q] = fmaf(ar, cs, t_acc[q]);
+            t_acc[q] = fmaf(-ai, sn, t_acc[q]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        if (FP64) dacc[q] += e_acc[q];
+        else kahan_add(ks[q], kc[q], t_acc[q]);
+      }
+      if (lane == 0) evaluated += ev;
+    }
+    __syncthreads();
+    if (s_abort) {
+      if (tid == 0 && it + 1 < ntile) mbar_wait_bounded(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
+      break;
+    }
+  }
+
+  if (p.counter && lane == 0 && evaluated && tile_ok) atomicAdd(p.counter, evaluated);
+  if (!tile_ok) return;
+  double *out = p.part + static_cast<long long>(blockIdx.y) * p.Jpad;
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const long long j = pbase + q * 32 + lane;
+    out[j] = FP64 ? dacc[q] : static_cast<double>(ks[q]) - static_cast<double>(kc[q]);
+  }
+}
+
+__global__ void k_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
+                             float scale, float *img, int accumulate) {
+  const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= J) return;
+  double s = 0;
+  for (int c = 0; c < nchunk; ++c) s += part[static_cast<long long>(c) * Jpad + j];
+  s *= static_cast<double>(scale);
+  if (accumulate) s += static_cast<double>(img[j]);
+  img[j] = static_cast<float>(s);
+}
+
+}  // namespace viss
+
+// ---------------------------------------------------------------- launchers
+namespace viss {
+
+// Launch shapes (template instances); the plan's tuner picks among these.
+constexpr int kFwdNT = 256;
+constexpr int kAdjNT = 256;
+
+template <int R, bool M, bool F>
+static cudaError_t fwd_inst(const FwdParams &p, int nchunk, cudaStream_t st) {
+  const long long per = static_cast<long long>(kFwdNT) * R;
+  const unsigned gx = static_cast<unsigned>((p.K + per - 1) / per);
+  dim3 grid(gx, nchunk);
+  k_forward<kFwdNT, R, M, F><<<grid, kFwdNT, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <int R>
+static cudaError_t fwd_dispatch(const FwdParams &p, int nchunk, bool masked, bool fp64,
+                                cudaStream_t st) {
+  if (fp64) return masked ? fwd_inst<R, true, true>(p, nchunk, st) : fwd_inst<R, false, true>(p, nchunk, st);
+  return masked ? fwd_inst<R, true, false>(p, nchunk, st) : fwd_inst<R, false, false>(p, nchunk, st);
+}
+
+cudaError_t launch_forward(const FwdParams &p, int R, int nchunk, bool masked, bool fp64,
+                           cudaStream_t st) {
+  if (p.K <= 0 || p.ntiles <= 0) return cudaSuccess;
+  if (fp64) return fwd_dispatch<2>(p, nchunk, masked, true, st);
+  switch (R) {
+    case 2: return fwd_dispatch<2>(p, nchunk, masked, false, st);
+    case 8: return fwd_dispatch<8>(p, nchunk, masked, false, st);
+    default: return fwd_dispatch<4>(p, nchunk, masked, false, st);
+  }
+}
+
+int forward_samples_per_block(int R, bool fp64) { return kFwdNT * (fp64 ? 2 : R); }
+
+cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
+                              cudaStream_t st) {
+  if (K <= 0) return cudaSuccess;
+  k_reduce_fwd<<<static_cast<unsigned>((K + 255) / 256), 256, 0, st>>>(K, nchunk, part, V, acc);
+  return cudaGetLastError();
+}
+
+template <bool M, bool F>
+static cudaError_t adj_inst(const AdjParams &p, int nchunk, cudaStream_t st) {
+  const long long pix_per_cta = static_cast<long long>(kAdjNT / 32) * kTilePix;
+  const unsigned gx = static_cast<unsigned>((p.Jpad + pix_per_cta - 1) / pix_per_cta);
+  dim3 grid(gx, nchunk);
+  k_adjoint<kAdjNT, kTilePix / 32, M, F><<<grid, kAdjNT, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint(const AdjParams &p, int nchunk, bool masked, bool fp64,
+                           cudaStream_t st) {
+  if (p.K <= 0 || p.Jpad <= 0) return cudaSuccess;
+  if (fp64) return masked ? adj_inst<true, true>(p, nchunk, st) : adj_inst<false, true>(p, nchunk, st);
+  return masked ? adj_inst<true, false>(p, nchunk, st) : adj_inst<false, false>(p, nchunk, st);
+}
+
+cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
+                              float scale, float *img, int acc, cudaStream_t st) {
+  if (J <= 0) return cudaSuccess;
+  k_reduce_adj<<<static_cast<unsigned>((J + 255) / 256), 256, 0, st>>>(J, Jpad, nchunk, part,
+                                                                        scale, img, acc);
+  return cudaGetLastError();
+}
+
+}  // namespace viss

@@ -1,0 +1,52 @@
+// visibility.cuh -- parameter blocks and launchers of the forward / adjoint
+// kernels (visibility.cu), shared with the C ABI layer (capi.cu).
+#pragma once
+
+#include "viss_common.cuh"
+
+namespace viss {
+
+constexpr int kSampTile = 128;  // samples per adjoint staging tile
+
+struct FwdParams {
+  const double4 *samp;   // [K] (u, v, w, off)
+  const int4 *refs;      // [K] occulter rows or null
+  const double4 *occ;    // [G]
+  const double4 *pix;    // [Jpad] (l, m, n, sky bits in the low word)
+  const double4 *cones;  // [ntiles]
+  long long K;
+  int ntiles;
+  int tiles_per_chunk;
+  double2 *part;                // [nchunk][K]
+  unsigned long long *counter;  // exponentials evaluated
+  int *err;
+  int use_off;                  // add the per-sample offset (.w) to the phase
+};
+
+struct AdjParams {
+  const double4 *samp;   // [K] (u, v, w, off)
+  const float2 *coef;    // [Kpad] plan-owned copy, padded to an even count
+  const int4 *refs;      // [K] or null
+  const double4 *occ;
+  const double4 *pix;    // [Jpad] (l, m, n, -)
+  const double4 *cones;  // [ntiles]
+  long long K;
+  long long Jpad;
+  int samples_per_chunk;  // multiple of kSampTile
+  double *part;           // [nchunk][Jpad]
+  unsigned long long *counter;
+  int *err;
+  int use_off;                  // add the per-sample offset (.w) to the phase
+};
+
+cudaError_t launch_forward(const FwdParams &p, int R, int nchunk, bool masked, bool fp64,
+                           cudaStream_t st);
+int forward_samples_per_block(int R, bool fp64);
+cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
+                              cudaStream_t st);
+cudaError_t launch_adjoint(const AdjParams &p, int nchunk, bool masked, bool fp64,
+                           cudaStream_t st);
+cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
+                              float scale, float *img, int acc, cudaStream_t st);
+
+}  // namespace viss
