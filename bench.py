@@ -31,6 +31,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "c3_10mhz"
+WORKLOAD_TEXT = {
+    "c3_10mhz": "Nside 256 (786,432 px) x 388,800 uvw samples (45 baselines x 8,640 snapshots), "
+                "10 MHz, Moon + Earth occultation",
+    "c3_1mhz": "Nside 256 (786,432 px) x 388,800 uvw samples (45 baselines x 8,640 snapshots), "
+               "1 MHz, Moon + Earth occultation",
+    "c2": "Nside 64 (49,152 px) x 20,160 uvw samples (28 baselines x 720 snapshots), 10 MHz, "
+          "Moon occultation (profiling-size case)",
+}
 METRIC = "G uvw x pixel terms/s (vis-gen + adjoint), split precision, rel-L2<=1e-5 vs FP64"
 UNIT = "Gterms/s"
 MUFU_TERMS_PER_CLK_PER_SM = 8     # 16 MUFU results/clk/SM, sin + cos per term
@@ -108,7 +116,7 @@ def run_ours(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    cfg = synth.CONFIGS[WORKLOAD]
+    cfg = synth.CONFIGS[args.workload]
     if world > 1:
         import dataclasses
         cfg = dataclasses.replace(cfg, day=float(rank))     # one observation day per replica
@@ -237,8 +245,7 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64-phase/f32-sincos",
         "data": "synthetic (seeded lunar-orbit formation and log-normal sky, see synth.py)",
-        "config": {"workload": "Nside 256 (786,432 px) x 388,800 uvw samples (45 baselines x "
-                               "8,640 snapshots), 10 MHz, Moon + Earth occultation",
+        "config": {"workload": WORKLOAD_TEXT.get(args.workload, args.workload),
                    "pixels": J, "samples": K, "terms_per_step": terms_per_step,
                    "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -345,6 +352,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOAD_TEXT),
+                    help="benchmark configuration (default: the headline one)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

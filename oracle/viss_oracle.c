@@ -31,6 +31,7 @@
  */
 #define _GNU_SOURCE
 #include <math.h>
+#include <quadmath.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -151,28 +152,34 @@ static void orc_nest_geo(int64_t nside, int64_t p, orc_pixgeo *g)
     g->kshift = kshift;
 }
 
-/* Long-double angles and unit vector of one pixel centre. */
-static void orc_geo_angles(int64_t nside, const orc_pixgeo *g, long double *theta,
-                           long double *phi, long double v[3])
+/* Angles and unit vector of one pixel centre in quad precision (113-bit
+ * significand), so that rounding to double is the correctly rounded value
+ * (double rounding is then astronomically unlikely).  cos(phi) and sin(phi)
+ * are exactly zero where phi is a multiple of pi/2. */
+static void orc_geo_angles(int64_t nside, const orc_pixgeo *g, __float128 *theta,
+                           __float128 *phi, __float128 v[3])
 {
-    const long double N = (long double)nside;
-    long double z, sth;
+    const __float128 N = (__float128)nside;
+    __float128 z, sth;
     if (g->polar != 0) {
         /* 1 - |z| = nr^2 / (3 N^2): exact rational, no cancellation */
-        long double omz = ((long double)g->nr * (long double)g->nr) / (3.0L * N * N);
-        sth = sqrtl(omz * (2.0L - omz));
-        z = (g->polar > 0) ? 1.0L - omz : omz - 1.0L;
-        long double half = 2.0L * asinl(sqrtl(omz * 0.5L));      /* angle from the pole */
-        *theta = (g->polar > 0) ? half : ORC_PI_L - half;
+        __float128 omz = ((__float128)g->nr * (__float128)g->nr) / (3 * N * N);
+        sth = sqrtq(omz * (2 - omz));
+        z = (g->polar > 0) ? 1 - omz : omz - 1;
+        __float128 half = 2 * asinq(sqrtq(omz / 2));      /* angle from the pole */
+        *theta = (g->polar > 0) ? half : M_PIq - half;
     } else {
-        z = (2.0L * N - (long double)g->iring) * 2.0L / (3.0L * N);
-        sth = sqrtl((1.0L - z) * (1.0L + z));
-        *theta = acosl(z);
+        z = (2 * N - (__float128)g->iring) * 2 / (3 * N);
+        sth = sqrtq((1 - z) * (1 + z));
+        *theta = acosq(z);
     }
-    long double q = (long double)(2 * g->jp - g->kshift - 1) / (long double)(4 * g->nr);
-    *phi = q * ORC_PI_L;
-    v[0] = sth * cosl(*phi);
-    v[1] = sth * sinl(*phi);
+    const int64_t num = 2 * g->jp - g->kshift - 1, den = 4 * g->nr;   /* phi = pi num/den */
+    *phi = M_PIq * (__float128)num / (__float128)den;
+    __float128 c = cosq(*phi), sn = sinq(*phi);
+    if ((2 * num) % den == 0 && ((2 * num / den) & 1)) c = 0;        /* phi = pi/2 + k pi */
+    if (num % den == 0) sn = 0;                                      /* phi = k pi */
+    v[0] = sth * c;
+    v[1] = sth * sn;
     v[2] = z;
 }
 
@@ -191,7 +198,7 @@ int orc_pix2ang(int nside, int scheme, int64_t first, int64_t count, double *the
         orc_pixgeo g;
         if (scheme == 0) orc_ring_geo(nside, first + i, &g);
         else orc_nest_geo(nside, first + i, &g);
-        long double th, ph, v[3];
+        __float128 th, ph, v[3];
         orc_geo_angles(nside, &g, &th, &ph, v);
         if (theta) theta[i] = (double)th;
         if (phi) phi[i] = (double)ph;

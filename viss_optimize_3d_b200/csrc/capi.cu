@@ -26,10 +26,13 @@ cudaError_t launch_occulters(long long, const double *, double, int, double, dou
                              cudaStream_t);
 cudaError_t launch_mask_bits(long long, long long, const double *, const int32_t *,
                              const double4 *, uint32_t *, cudaStream_t);
-cudaError_t launch_stage_pixels(long long, long long, const double *, double4 *, double4 *,
-                                cudaStream_t);
-cudaError_t launch_stage_sky(long long, long long, const double4 *, const float *, float,
-                             double4 *, cudaStream_t);
+cudaError_t launch_pix_keys(long long, const double *, unsigned long long *, int *, cudaStream_t);
+cudaError_t sort_pixel_keys(long long, unsigned long long *, unsigned long long *, int *, int *,
+                            cudaStream_t);
+cudaError_t launch_stage_pixels(long long, long long, const double *, const int *, double4 *,
+                                double4 *, cudaStream_t);
+cudaError_t launch_stage_sky(long long, long long, const double4 *, const int *, const float *,
+                             float, double4 *, cudaStream_t);
 cudaError_t launch_stage_coef(long long, long long, const float2 *, float2 *, cudaStream_t);
 cudaError_t launch_stage_samples(long long, const double *, const double *, const int32_t *,
                                  double4 *, int4 *, unsigned long long *, cudaStream_t);
@@ -100,6 +103,7 @@ struct viss_plan {
   double4 *pix = nullptr;    size_t pix_cap = 0;
   double4 *pixsky = nullptr; size_t pixsky_cap = 0;
   double4 *cones = nullptr;  size_t cones_cap = 0;
+  int *perm = nullptr;       size_t perm_cap = 0;  // record i holds caller pixel perm[i]
   // samples
   long long K = 0, Kpad = 0;
   double4 *samp = nullptr; size_t samp_cap = 0;
@@ -284,7 +288,8 @@ int viss_plan_create(viss_plan **plan) {
 
 int viss_plan_destroy(viss_plan *p) {
   if (!p) return VISS_OK;
-  void *bufs[] = {p->pix, p->pixsky, p->cones, p->samp, p->refs, p->occ, p->coef, p->part, p->dev_words};
+  void *bufs[] = {p->pix, p->pixsky, p->cones, p->perm, p->samp, p->refs, p->occ, p->coef, p->part,
+                  p->dev_words};
   for (void *b : bufs)
     if (b) cudaFree(b);
   delete p;
@@ -300,7 +305,20 @@ int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *strea
   if (int s = ensure(p->pix, p->pix_cap, sizeof(double4) * Jpad, "pixel records")) return s;
   if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * Jpad, "pixel+sky records")) return s;
   if (int s = ensure(p->cones, p->cones_cap, sizeof(double4) * nt, "tile cones")) return s;
-  VISS_CUDA(viss::launch_stage_pixels(J, Jpad, lmn, p->pix, p->cones, as_stream(stream)),
+  if (int s = ensure(p->perm, p->perm_cap, sizeof(int) * J, "pixel order")) return s;
+  const cudaStream_t st = as_stream(stream);
+  // compact tiles: order the pixels by a hierarchical (NESTED) locality key
+  void *tmp = nullptr;
+  const size_t kbytes = sizeof(unsigned long long) * J, ibytes = sizeof(int) * J;
+  VISS_CUDA(cudaMallocAsync(&tmp, 2 * kbytes + ibytes, st), "viss_plan_set_pixels: keys");
+  auto *keys = static_cast<unsigned long long *>(tmp);
+  auto *idx = reinterpret_cast<int *>(keys + 2 * J);
+  cudaError_t e = viss::launch_pix_keys(J, lmn, keys, idx, st);
+  if (e == cudaSuccess) e = viss::sort_pixel_keys(J, keys, keys + J, idx, p->perm, st);
+  cudaError_t e2 = cudaFreeAsync(tmp, st);
+  if (e != cudaSuccess) return cuda_fail(e, "viss_plan_set_pixels: order");
+  if (e2 != cudaSuccess) return cuda_fail(e2, "viss_plan_set_pixels: free");
+  VISS_CUDA(viss::launch_stage_pixels(J, Jpad, lmn, p->perm, p->pix, p->cones, st),
             "viss_plan_set_pixels");
   p->J = J;
   p->Jpad = Jpad;
@@ -360,7 +378,8 @@ int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stre
   const int R = fp64 ? 2 : p->fwd_R;
   const int nchunk = fwd_chunks(p, R, fp64);
   if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * p->K)) return s;
-  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, sky, 1.0f, p->pixsky, st), "viss_forward: sky");
+  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, st),
+            "viss_forward: sky");
   VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 2 * sizeof(unsigned long long), st), "viss_forward");
   viss::FwdParams fp;
   fp.samp = p->samp;
@@ -414,7 +433,7 @@ int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int
   ap.err = reinterpret_cast<int *>(p->dev_words + 1);
   ap.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
   VISS_CUDA(viss::launch_adjoint(ap, nchunk, masked, fp64, st), "viss_adjoint: kernel");
-  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, ap.part, scale, image,
+  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, ap.part, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_adjoint: reduce");
   p->last_total = p->K * p->J;

@@ -8,6 +8,8 @@
 // fixed operation order (dot_exact) so that the CPU oracle reproduces every
 // bit; the same form with thr = -sqrt(1 - (R/|P|)^2) is the exact ray-sphere
 // test, and with q = -e, thr = -cos(rho) an Earth cap of radius rho.
+#include <cub/device/device_radix_sort.cuh>
+
 #include "viss_common.cuh"
 
 namespace viss {
@@ -57,13 +59,63 @@ __global__ void k_mask_bits(long long K, long long J, const double *lmn, const i
   if (lane == 0) bits[word] = b;
 }
 
-// Pixel staging: lmn (J x 3) -> double4 records, padded to Jpad with copies
-// of the last pixel (they never reach an output: sky is zero there and the
-// adjoint drops them).
-__global__ void k_stage_pixels(long long J, long long Jpad, const double *lmn, double4 *pix) {
+// Locality key of a direction: its HEALPix NESTED index at Nside 2^13
+// (standard ang2pix_nest).  NESTED indices are hierarchical, so sorting by the
+// key puts every 4^k-aligned run of pixels in a compact patch of sky -- for a
+// HEALPix grid of any Nside <= 2^13 the sorted order is its NESTED order.
+__device__ unsigned long long spread32(unsigned long long x) {
+  x &= 0xffffffffull;
+  x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+  x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
+}
+
+__global__ void k_pix_keys(long long J, const double *lmn, unsigned long long *keys, int *idx) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= J) return;
+  const long long N = 8192;
+  const double x = lmn[3 * i], y = lmn[3 * i + 1], z0 = lmn[3 * i + 2];
+  const double r = sqrt(x * x + y * y + z0 * z0);
+  const double z = r > 0 ? z0 / r : 1.0;
+  const double za = fabs(z);
+  double phi = atan2(y, x);
+  if (phi < 0) phi += 2.0 * 3.141592653589793;
+  double tt = phi / (0.5 * 3.141592653589793);
+  if (tt >= 4.0) tt -= 4.0;
+  long long face, ix, iy;
+  if (za <= 2.0 / 3.0) {
+    const double t1 = N * (0.5 + tt), t2 = N * z * 0.75;
+    const long long jp = static_cast<long long>(t1 - t2), jm = static_cast<long long>(t1 + t2);
+    const long long ifp = jp / N, ifm = jm / N;
+    face = (ifp == ifm) ? (ifp | 4) : ((ifp < ifm) ? ifp : ifm + 8);
+    ix = jm & (N - 1);
+    iy = N - (jp & (N - 1)) - 1;
+  } else {
+    const long long ntt = min(3LL, static_cast<long long>(tt));
+    const double tp = tt - ntt;
+    const double tmp = N * sqrt(3.0 * (1.0 - za));
+    const long long jp = min(N - 1, static_cast<long long>(tp * tmp));
+    const long long jm = min(N - 1, static_cast<long long>((1.0 - tp) * tmp));
+    if (z >= 0) { face = ntt; ix = N - jm - 1; iy = N - jp - 1; }
+    else { face = ntt + 8; ix = jp; iy = jm; }
+  }
+  face = face < 0 ? 0 : (face > 11 ? 11 : face);
+  ix = ix < 0 ? 0 : (ix >= N ? N - 1 : ix);
+  iy = iy < 0 ? 0 : (iy >= N ? N - 1 : iy);
+  keys[i] = static_cast<unsigned long long>(face) * N * N + spread32(ix) + (spread32(iy) << 1);
+  idx[i] = static_cast<int>(i);
+}
+
+// Pixel staging: record i = pixel perm[i] of lmn (J x 3); padded to Jpad with
+// copies of the last record (sky is zero there and the adjoint drops them).
+__global__ void k_stage_pixels(long long J, long long Jpad, const double *lmn, const int *perm,
+                               double4 *pix) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= Jpad) return;
-  const long long s = i < J ? i : J - 1;
+  const long long s = perm[i < J ? i : J - 1];
   pix[i] = make_double4(lmn[3 * s], lmn[3 * s + 1], lmn[3 * s + 2], 0.0);
 }
 
@@ -101,12 +153,12 @@ __global__ void k_tile_cones(long long ntiles, const double4 *pix, double4 *cone
 
 // Sky staging: pixel record + sky value in the low word of .w (zero past J),
 // so one 32-byte record per pixel carries everything the forward reads.
-__global__ void k_stage_sky(long long J, long long Jpad, const double4 *pix, const float *sky,
-                            float scale, double4 *out) {
+__global__ void k_stage_sky(long long J, long long Jpad, const double4 *pix, const int *perm,
+                            const float *sky, float scale, double4 *out) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= Jpad) return;
   double4 r = pix[i];
-  const float v = i < J ? __fmul_rn(sky[i], scale) : 0.0f;
+  const float v = i < J ? __fmul_rn(sky[perm[i]], scale) : 0.0f;
   r.w = __hiloint2double(0, __float_as_int(v));
   out[i] = r;
 }
@@ -158,9 +210,16 @@ cudaError_t launch_mask_bits(long long K, long long J, const double *lmn, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, double4 *pix,
-                                double4 *cones, cudaStream_t st) {
-  k_stage_pixels<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, lmn, pix);
+cudaError_t launch_pix_keys(long long J, const double *lmn, unsigned long long *keys, int *idx,
+                            cudaStream_t st) {
+  if (J <= 0) return cudaSuccess;
+  k_pix_keys<<<nblk(J, 256), 256, 0, st>>>(J, lmn, keys, idx);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, const int *perm,
+                                double4 *pix, double4 *cones, cudaStream_t st) {
+  k_stage_pixels<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, lmn, perm, pix);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const long long nt = Jpad / kTilePix;
@@ -168,9 +227,9 @@ cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage_sky(long long J, long long Jpad, const double4 *pix, const float *sky,
-                             float scale, double4 *out, cudaStream_t st) {
-  k_stage_sky<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, pix, sky, scale, out);
+cudaError_t launch_stage_sky(long long J, long long Jpad, const double4 *pix, const int *perm,
+                             const float *sky, float scale, double4 *out, cudaStream_t st) {
+  k_stage_sky<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, pix, perm, sky, scale, out);
   return cudaGetLastError();
 }
 
@@ -198,6 +257,22 @@ cudaError_t launch_stage_samples(long long K, const double *uvw, const double *o
   if (e != cudaSuccess || !bound) return e;
   k_sample_bound<<<nblk(K, 256), 256, 0, st>>>(K, samp, bound);
   return cudaGetLastError();
+}
+
+// Sort (key, index) pairs by key: the plan's pixel order.  Plan set-up only.
+cudaError_t sort_pixel_keys(long long J, unsigned long long *keys_in, unsigned long long *keys_out,
+                            int *idx_in, int *idx_out, cudaStream_t st) {
+  size_t temp = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, keys_in, keys_out, idx_in, idx_out,
+                                                  static_cast<int>(J), 0, 50, st);
+  if (e != cudaSuccess) return e;
+  void *tmp = nullptr;
+  e = cudaMallocAsync(&tmp, temp, st);
+  if (e != cudaSuccess) return e;
+  e = cub::DeviceRadixSort::SortPairs(tmp, temp, keys_in, keys_out, idx_in, idx_out,
+                                      static_cast<int>(J), 0, 50, st);
+  cudaError_t e2 = cudaFreeAsync(tmp, st);
+  return e != cudaSuccess ? e : e2;
 }
 
 }  // namespace viss

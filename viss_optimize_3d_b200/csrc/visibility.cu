@@ -45,24 +45,37 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   s = t;
 }
 
-// State of a sample (3 occulter refs) against a tile cone: min over refs of
-// cone_state (2 all visible, 0 none, 1 mixed).
+// Classification of a sample (3 occulter refs) against a tile cone, packed:
+// bits 0-1 state (2 every pixel visible, 0 none, 1 mixed), bits 2-4 which
+// refs are mixed on this tile (only those need the per-pixel test).
 __device__ __forceinline__ int sample_state(const int4 &rf, const double4 &cone,
                                             const double4 *occ) {
-  int st = 2;
-  if (rf.x >= 0) st = min(st, cone_state(cone, occ[rf.x]));
-  if (rf.y >= 0) st = min(st, cone_state(cone, occ[rf.y]));
-  if (rf.z >= 0) st = min(st, cone_state(cone, occ[rf.z]));
-  return st;
+  int st = 2, need = 0;
+  const int r3[3] = {rf.x, rf.y, rf.z};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (r3[c] < 0) continue;
+    const int s = cone_state(cone, occ[r3[c]]);
+    st = min(st, s);
+    if (s == 1) need |= 1 << c;
+  }
+  return st == 1 ? (1 | (need << 2)) : st;
 }
 
-__device__ __forceinline__ bool visible_exact(const int4 &rf, const double4 *occ, double s0,
-                                              double s1, double s2) {
-  bool v = true;
-  if (rf.x >= 0) { const double4 q = occ[rf.x]; v = v && (dot_exact(s0, s1, s2, q) >= q.w); }
-  if (rf.y >= 0) { const double4 q = occ[rf.y]; v = v && (dot_exact(s0, s1, s2, q) >= q.w); }
-  if (rf.z >= 0) { const double4 q = occ[rf.z]; v = v && (dot_exact(s0, s1, s2, q) >= q.w); }
-  return v;
+// The occulter rows a mixed sample must test; rows it need not test become a
+// row every direction passes (thr = -4 < any dot of unit vectors).
+__device__ __forceinline__ void mixed_rows(const int4 &rf, int code, const double4 *occ,
+                                           double4 &q0, double4 &q1, double4 &q2) {
+  const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
+  q0 = (code & 4) ? occ[rf.x] : pass;
+  q1 = (code & 8) ? occ[rf.y] : pass;
+  q2 = (code & 16) ? occ[rf.z] : pass;
+}
+
+__device__ __forceinline__ bool visible_rows(const double4 &q0, const double4 &q1,
+                                             const double4 &q2, double s0, double s1, double s2) {
+  return (dot_exact(s0, s1, s2, q0) >= q0.w) & (dot_exact(s0, s1, s2, q1) >= q1.w) &
+         (dot_exact(s0, s1, s2, q2) >= q2.w);
 }
 
 __device__ __forceinline__ float sky_of(const double4 &p) {
@@ -153,7 +166,7 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
         if (kval[r]) {
           st[r] = sample_state(rf[r], cone, p.occ);
           full = full && (st[r] == 2);
-          any = any || (st[r] != 0);
+          any = any || ((st[r] & 3) != 0);
         }
       }
       const bool wfull = __all_sync(0xffffffffu, full);
@@ -193,13 +206,16 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
           }
         }
       } else {
-        for (int j = 0; j < kTilePix; ++j) {
-          const double4 q = tp[j];
-          const float I = sky_of(q);
+        // mixed tile: one sample at a time, its occulter rows in registers
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const bool vis = st[r] == 2 || (st[r] == 1 && visible_exact(rf[r], p.occ, q.x, q.y, q.z));
-            const float Iv = vis ? I : 0.f;
+        for (int r = 0; r < R; ++r) {
+          if ((st[r] & 3) == 0) continue;
+          double4 q0, q1, q2;
+          mixed_rows(rf[r], st[r], p.occ, q0, q1, q2);
+          for (int j = 0; j < kTilePix; ++j) {
+            const double4 q = tp[j];
+            const bool vis = visible_rows(q0, q1, q2, q.x, q.y, q.z);
+            const float Iv = vis ? sky_of(q) : 0.f;
             const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
             if (FP64) {
               double sn, cs;
@@ -356,18 +372,19 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
       for (int q = 0; q < P; ++q) { t_acc[q] = 0.f; e_acc[q] = 0.0; }
       for (int i = 0; i < gn; ++i) {
         const int sst = MASKED ? __shfl_sync(0xffffffffu, st, i) : 2;
-        if (sst == 0) continue;
+        if ((sst & 3) == 0) continue;
         ev += kTilePix;
         const double4 u = sp[g + i];
         const float2 a = cp[g + i];
         const double uoff = p.use_off ? u.w : 0.0;
         const double m = FP64 ? uoff : kMagic + uoff;
-        int4 rfi;
-        if (MASKED && sst == 1) rfi = s_refs[buf][g + i];
+        const bool mixed = MASKED && (sst & 3) == 1;
+        double4 q0, q1, q2;
+        if (mixed) mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
 #pragma unroll
         for (int q = 0; q < P; ++q) {
           bool vis = true;
-          if (MASKED && sst == 1) vis = visible_exact(rfi, p.occ, sx[q], sy[q], sz[q]);
+          if (mixed) vis = visible_rows(q0, q1, q2, sx[q], sy[q], sz[q]);
           const double t = fma(u.z, sz[q], fma(u.y, sy[q], fma(u.x, sx[q], m)));
           if (FP64) {
             double sn, cs;
@@ -407,13 +424,15 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
   }
 }
 
+// image[perm[i]] = scale * sum over chunks of record i (FP64).
 __global__ void k_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
-                             float scale, float *img, int accumulate) {
-  const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (j >= J) return;
+                             const int *perm, float scale, float *img, int accumulate) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= J) return;
   double s = 0;
-  for (int c = 0; c < nchunk; ++c) s += part[static_cast<long long>(c) * Jpad + j];
+  for (int c = 0; c < nchunk; ++c) s += part[static_cast<long long>(c) * Jpad + i];
   s *= static_cast<double>(scale);
+  const long long j = perm[i];
   if (accumulate) s += static_cast<double>(img[j]);
   img[j] = static_cast<float>(s);
 }
@@ -480,10 +499,10 @@ cudaError_t launch_adjoint(const AdjParams &p, int nchunk, bool masked, bool fp6
 }
 
 cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
-                              float scale, float *img, int acc, cudaStream_t st) {
+                              const int *perm, float scale, float *img, int acc, cudaStream_t st) {
   if (J <= 0) return cudaSuccess;
   k_reduce_adj<<<static_cast<unsigned>((J + 255) / 256), 256, 0, st>>>(J, Jpad, nchunk, part,
-                                                                        scale, img, acc);
+                                                                        perm, scale, img, acc);
   return cudaGetLastError();
 }
 

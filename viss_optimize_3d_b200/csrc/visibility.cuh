@@ -47,6 +47,6 @@ cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, floa
 cudaError_t launch_adjoint(const AdjParams &p, int nchunk, bool masked, bool fp64,
                            cudaStream_t st);
 cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
-                              float scale, float *img, int acc, cudaStream_t st);
+                              const int *perm, float scale, float *img, int acc, cudaStream_t st);
 
 }  // namespace viss
