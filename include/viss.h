@@ -137,6 +137,10 @@ int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, 
  * (visible-or-mixed pairs actually exponentiated) and the total K*J, read
  * back from the device (synchronises the plan's last stream). */
 int viss_plan_last_counts(viss_plan *plan, int64_t *evaluated, int64_t *total);
+/* The same plus the terms evaluated in "mixed" tiles (per-term occultation
+ * test).  Returns VISS_ERR_TIMEOUT if the last kernel reported a bounded
+ * staging wait that gave up. */
+int viss_plan_last_stats(viss_plan *plan, int64_t *evaluated, int64_t *mixed, int64_t *total);
 
 /* ----------------------------------------------- density compensation
  * Replaces ceilAndScale + countOccurrences + calculateR + calculateDcf

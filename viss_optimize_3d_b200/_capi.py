@@ -60,6 +60,7 @@ _SIGS = {
     "viss_forward": (_i, [_v, _v, _v, _i, _v]),
     "viss_adjoint": (_i, [_v, _v, _v, _f, _i, _v]),
     "viss_plan_last_counts": (_i, [_v, C.POINTER(_i64), C.POINTER(_i64)]),
+    "viss_plan_last_stats": (_i, [_v, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "viss_dcf": (_i, [_i64, _v, _i, _i, _v, _v, _v, _v]),
     "viss_weights": (_i, [_i64, _v, _v, _v, _v, _i, _v, _v, _v]),
     "viss_wrot": (_i, [_i64, _v, _v, _v]),

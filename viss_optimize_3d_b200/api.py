@@ -202,6 +202,13 @@ class Plan:
         check(lib.viss_plan_last_counts(self._h, C.byref(ev), C.byref(tot)), "viss_plan_last_counts")
         return ev.value, tot.value
 
+    def last_stats(self):
+        """(evaluated, evaluated in mixed tiles, K*J) of the last call (syncs)."""
+        ev, mx, tot = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.viss_plan_last_stats(self._h, C.byref(ev), C.byref(mx), C.byref(tot)),
+              "viss_plan_last_stats")
+        return ev.value, mx.value, tot.value
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             lib.viss_plan_destroy(self._h)

@@ -115,12 +115,15 @@ struct viss_plan {
   double max_turns = 0;
   // workspace + device status words
   void *part = nullptr;    size_t part_cap = 0;
-  unsigned long long *dev_words = nullptr;  // [0] evaluated counter, [1] error flags, [2] bound
+  // [0] terms evaluated, [1] error flags, [2] terms evaluated in mixed tiles,
+  // [3] |u|+|v|+|w|+|off| bound of the staged samples
+  unsigned long long *dev_words = nullptr;
   size_t dev_words_cap = 0;
   long long last_total = 0;
   cudaStream_t last_stream = nullptr;
   // launch shape
   int fwd_R = 4;
+  int adj_P = 8;
   int fwd_waves = 16;
   int adj_waves = 16;
 };
@@ -137,7 +140,7 @@ int fwd_chunks(const viss_plan *p, int R, bool fp64) {
 }
 
 int adj_chunks(const viss_plan *p, bool fp64, int *samples_per_chunk) {
-  const long long per = 8LL * viss::kTilePix;  // pixels per CTA
+  const long long per = viss::adjoint_pixels_per_block(p->adj_P, fp64);  // pixels per CTA
   const long long blocks = (p->Jpad + per - 1) / per;
   const long long slots = static_cast<long long>(p->nsm) * (fp64 ? 1 : 2);
   long long c = (static_cast<long long>(p->adj_waves) * slots + blocks - 1) / blocks;
@@ -300,7 +303,8 @@ int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *strea
   if (!p || J <= 0 || !lmn) return fail(VISS_ERR_ARG, "viss_plan_set_pixels: bad arguments");
   if (J > (1LL << 31) * viss::kTilePix / 2)
     return fail(VISS_ERR_ARG, "viss_plan_set_pixels: too many pixels");
-  const long long Jpad = (J + viss::kTilePix - 1) / viss::kTilePix * viss::kTilePix;
+  // whole warp tiles of the adjoint (2 cone tiles = 256 pixels)
+  const long long Jpad = (J + 2 * viss::kTilePix - 1) / (2 * viss::kTilePix) * (2 * viss::kTilePix);
   const long long nt = Jpad / viss::kTilePix;
   if (int s = ensure(p->pix, p->pix_cap, sizeof(double4) * Jpad, "pixel records")) return s;
   if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * Jpad, "pixel+sky records")) return s;
@@ -342,13 +346,13 @@ int viss_plan_set_samples(viss_plan *p, int64_t K, const double *uvw, const doub
     VISS_CUDA(cudaMemcpyAsync(p->occ, occ, sizeof(double4) * G, cudaMemcpyDeviceToDevice, st),
               "viss_plan_set_samples: occulters");
   }
-  VISS_CUDA(cudaMemsetAsync(p->dev_words + 2, 0, sizeof(unsigned long long), st),
+  VISS_CUDA(cudaMemsetAsync(p->dev_words + 3, 0, sizeof(unsigned long long), st),
             "viss_plan_set_samples");
   VISS_CUDA(viss::launch_stage_samples(K, uvw, off, refs, p->samp, refs ? p->refs : nullptr,
-                                       p->dev_words + 2, st),
+                                       p->dev_words + 3, st),
             "viss_plan_set_samples");
   unsigned long long bits = 0;
-  VISS_CUDA(cudaMemcpyAsync(&bits, p->dev_words + 2, sizeof(bits), cudaMemcpyDeviceToHost, st),
+  VISS_CUDA(cudaMemcpyAsync(&bits, p->dev_words + 3, sizeof(bits), cudaMemcpyDeviceToHost, st),
             "viss_plan_set_samples: bound");
   VISS_CUDA(cudaStreamSynchronize(st), "viss_plan_set_samples: sync");
   double bound;
@@ -380,7 +384,7 @@ int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stre
   if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * p->K)) return s;
   VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, st),
             "viss_forward: sky");
-  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 2 * sizeof(unsigned long long), st), "viss_forward");
+  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_forward");
   viss::FwdParams fp;
   fp.samp = p->samp;
   fp.refs = masked ? p->refs : nullptr;
@@ -417,7 +421,7 @@ int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int
   if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->Jpad)) return s;
   VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
             "viss_adjoint: coef");
-  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 2 * sizeof(unsigned long long), st), "viss_adjoint");
+  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_adjoint");
   viss::AdjParams ap;
   ap.samp = p->samp;
   ap.coef = p->coef;
@@ -432,7 +436,7 @@ int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int
   ap.counter = p->dev_words;
   ap.err = reinterpret_cast<int *>(p->dev_words + 1);
   ap.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
-  VISS_CUDA(viss::launch_adjoint(ap, nchunk, masked, fp64, st), "viss_adjoint: kernel");
+  VISS_CUDA(viss::launch_adjoint(ap, p->adj_P, nchunk, masked, fp64, st), "viss_adjoint: kernel");
   VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, ap.part, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_adjoint: reduce");
@@ -441,16 +445,21 @@ int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int
   return VISS_OK;
 }
 
-int viss_plan_last_counts(viss_plan *p, int64_t *evaluated, int64_t *total) {
-  if (!p) return fail(VISS_ERR_ARG, "viss_plan_last_counts: null plan");
-  unsigned long long w[2] = {0, 0};
-  VISS_CUDA(cudaStreamSynchronize(p->last_stream), "viss_plan_last_counts: sync");
-  VISS_CUDA(cudaMemcpy(w, p->dev_words, sizeof(w), cudaMemcpyDeviceToHost), "viss_plan_last_counts");
+int viss_plan_last_stats(viss_plan *p, int64_t *evaluated, int64_t *mixed, int64_t *total) {
+  if (!p) return fail(VISS_ERR_ARG, "viss_plan_last_stats: null plan");
+  unsigned long long w[3] = {0, 0, 0};
+  VISS_CUDA(cudaStreamSynchronize(p->last_stream), "viss_plan_last_stats: sync");
+  VISS_CUDA(cudaMemcpy(w, p->dev_words, sizeof(w), cudaMemcpyDeviceToHost), "viss_plan_last_stats");
   if (evaluated) *evaluated = static_cast<int64_t>(w[0]);
+  if (mixed) *mixed = static_cast<int64_t>(w[2]);
   if (total) *total = p->last_total;
   if (w[1] & viss::kErrTimeout)
     return fail(VISS_ERR_TIMEOUT, "a bounded shared-memory staging wait gave up in the last kernel");
   return VISS_OK;
+}
+
+int viss_plan_last_counts(viss_plan *p, int64_t *evaluated, int64_t *total) {
+  return viss_plan_last_stats(p, evaluated, nullptr, total);
 }
 
 // --------------------------------------------------------------------- DCF

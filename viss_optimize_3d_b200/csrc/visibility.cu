@@ -5,11 +5,11 @@
 //   adjoint  C_j = sum_k Re(a_k exp(+2 pi i (u_k.s_j + off_k))) vis_kj
 //            replaces computeC (vissgen3d_blockage.cu:167-192)
 //
-// Both are matrix-free matvecs bound by the SFU (two MUFU ops per term:
-// sin and cos), not by HBM and not by tensor cores.  Per term the split path
-// issues: 3 DFMA (phase in FP64, already reduced to a 2^-23-turn fixed point
-// by the kMagic offset), 1 LOP3 (fraction -> float), 1 FFMA (-> radians),
-// sin/cos, 2 FFMA (accumulate).
+// Both are matrix-free matvecs bound by the SFU (two MUFU ops per term: sin
+// and cos), not by HBM and not by tensor cores.  Per term the split path
+// issues 3 DFMA (phase in FP64, already reduced to a 2^-23-turn fixed point by
+// the kMagic offset), 1 LOP3 (fraction -> float), 1 FFMA (-> radians), the
+// SFU's argument scaling, sin, cos and 2 FFMA (accumulate).
 //
 // Work decomposition
 //   forward: a CTA owns NT*R samples (R per thread, in registers) and one
@@ -18,24 +18,24 @@
 //            (TMA engine) and are read as warp-wide broadcasts.  Partial sums
 //            of each chunk go to a [chunk][K] FP64 workspace; k_reduce_fwd
 //            adds the chunks in FP64.
-//   adjoint: a warp owns one pixel tile (32 lanes x 4 pixels, in registers);
-//            a CTA owns 8 tiles and one chunk of samples, which stream through
-//            shared memory the same way.  Chunks go to a [chunk][J] FP64
-//            workspace reduced by k_reduce_adj.
-// Occultation: every tile carries a bounding cone (centre, chord radius).
-// Against a sample's occulters a tile is "all visible" (no per-term test),
-// "none visible" (skipped) or "mixed" (exact FP64 predicate per term, the
-// same operations as the CPU oracle, so the mask bits match it exactly).
-// The decision is warp-uniform: the warp votes in the forward, and in the
-// adjoint the sample is uniform across the warp.
+//   adjoint: a warp owns 32*P pixels (P per lane, in registers); a CTA owns
+//            NT/32 such warp tiles and one chunk of samples, which stream
+//            through shared memory the same way.  Chunks go to a [chunk][Jpad]
+//            FP64 workspace reduced (and un-permuted) by k_reduce_adj.
+// Occultation: every kTilePix-pixel tile carries a bounding cone (centre,
+// chord radius).  Against each of a sample's occulters a tile is "all
+// visible" (no per-term test), "none visible" (the sample skips the tile) or
+// "mixed" (the exact FP64 predicate per term, the same operations as the CPU
+// oracle, so the mask bits match it exactly).  The decision is warp-uniform:
+// the warp votes in the forward; in the adjoint the sample is uniform across
+// the warp.
 //
-// Accuracy: terms are summed in FP32 within a tile (<= 128 terms per
-// accumulator), tile sums are folded into a Kahan-compensated FP32 sum, and
-// chunks are added in FP64.
+// Accuracy: terms are summed in FP32 within a tile / sample group (<= 128
+// terms per accumulator), those partial sums are folded into a
+// Kahan-compensated FP32 sum, and chunks are added in FP64.
 #include "visibility.cuh"
 
 namespace viss {
-
 
 // Kahan-compensated add of x into (s, c).
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
@@ -45,7 +45,7 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   s = t;
 }
 
-// Classification of a sample (3 occulter refs) against a tile cone, packed:
+// Classification of a sample (3 occulter refs) against one tile cone, packed:
 // bits 0-1 state (2 every pixel visible, 0 none, 1 mixed), bits 2-4 which
 // refs are mixed on this tile (only those need the per-pixel test).
 __device__ __forceinline__ int sample_state(const int4 &rf, const double4 &cone,
@@ -60,6 +60,27 @@ __device__ __forceinline__ int sample_state(const int4 &rf, const double4 &cone,
     if (s == 1) need |= 1 << c;
   }
   return st == 1 ? (1 | (need << 2)) : st;
+}
+
+// The same against the union of two tiles (a warp tile of 256 pixels): hidden
+// only if hidden on both; all visible only if all visible on both; otherwise
+// every ref that is not all-visible on both tiles is tested per pixel.
+__device__ __forceinline__ int sample_state2(const int4 &rf, const double4 &c0,
+                                             const double4 &c1, const double4 *occ) {
+  const int a = sample_state(rf, c0, occ), b = sample_state(rf, c1, occ);
+  const int sa = a & 3, sb = b & 3;
+  if (sa == 0 && sb == 0) return 0;
+  if (sa == 2 && sb == 2) return 2;
+  int need = 0;
+  const int r3[3] = {rf.x, rf.y, rf.z};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (r3[c] < 0) continue;
+    const bool full0 = (sa == 2) || (sa == 1 && !((a >> (2 + c)) & 1));
+    const bool full1 = (sb == 2) || (sb == 1 && !((b >> (2 + c)) & 1));
+    if (!(full0 && full1)) need |= 1 << c;
+  }
+  return need ? (1 | (need << 2)) : 2;
 }
 
 // The occulter rows a mixed sample must test; rows it need not test become a
@@ -82,10 +103,27 @@ __device__ __forceinline__ float sky_of(const double4 &p) {
   return __int_as_float(__double2loint(p.w));
 }
 
-// FP64 reference term: (cos, sin) of 2 pi (phase mod 1), phase in FP64.
+// FP64 reference term: (sin, cos) of 2 pi (phase mod 1), phase in FP64.
 __device__ __forceinline__ void sincos_turns_fp64(double t, double &sn, double &cs) {
   const double f = t - rint(t);
   sincospi(2.0 * f, &sn, &cs);
+}
+
+// One forward term into (re, im): sky I at phase t.
+template <bool FP64>
+__device__ __forceinline__ void fwd_term(double t, float I, float &re, float &im, double &dre,
+                                         double &dim) {
+  if (FP64) {
+    double sn, cs;
+    sincos_turns_fp64(t, sn, cs);
+    dre = fma(static_cast<double>(I), cs, dre);
+    dim = fma(-static_cast<double>(I), sn, dim);
+  } else {
+    float sn, cs;
+    sfu_sincos(turn_angle(t), sn, cs);
+    re = fmaf(I, cs, re);
+    im = fmaf(-I, sn, im);
+  }
 }
 
 // ======================================================================
@@ -94,6 +132,7 @@ __device__ __forceinline__ void sincos_turns_fp64(double t, double &sn, double &
 template <int NT, int R, bool MASKED, bool FP64>
 __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p) {
   __shared__ __align__(128) double4 s_pix[2][kTilePix];
+  __shared__ __align__(16) int4 s_refs[MASKED ? R : 1][MASKED ? NT : 1];
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ int s_abort;
 
@@ -101,7 +140,6 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
   const long long kb = static_cast<long long>(blockIdx.x) * (NT * R);
 
   double ux[R], uy[R], uz[R], mk[R];
-  int4 rf[R];
   bool kval[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -111,9 +149,8 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
     ux[r] = s.x; uy[r] = s.y; uz[r] = s.z;
     const double off = p.use_off ? s.w : 0.0;
     mk[r] = FP64 ? off : kMagic + off;
-    if (MASKED) rf[r] = kval[r] ? p.refs[k] : make_int4(-1, -1, -1, -1);
+    if (MASKED) s_refs[r][tid] = kval[r] ? p.refs[k] : make_int4(-1, -1, -1, -1);
   }
-
   unsigned nval_warp = 0;  // valid samples of this warp
 #pragma unroll
   for (int r = 0; r < R; ++r) nval_warp += __popc(__ballot_sync(0xffffffffu, kval[r]));
@@ -143,7 +180,7 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
     bulk_g2s(s_pix[0], p.pix + static_cast<long long>(t0) * kTilePix, kTileBytes, &s_bar[0]);
   }
 
-  unsigned long long evaluated = 0;
+  unsigned long long evaluated = 0, mixed_terms = 0;
   int it = 0;
   for (int t = t0; t < t1; ++t, ++it) {
     const int buf = it & 1;
@@ -164,7 +201,7 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if (kval[r]) {
-          st[r] = sample_state(rf[r], cone, p.occ);
+          st[r] = sample_state(s_refs[r][tid], cone, p.occ);
           full = full && (st[r] == 2);
           any = any || ((st[r] & 3) != 0);
         }
@@ -179,7 +216,10 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
     }
     const double4 *tp = s_pix[buf];
     if (mode != 0) {
-      if ((tid & 31) == 0) evaluated += static_cast<unsigned long long>(nval_warp) * kTilePix;
+      if ((tid & 31) == 0) {
+        evaluated += static_cast<unsigned long long>(nval_warp) * kTilePix;
+        if (mode == 1) mixed_terms += static_cast<unsigned long long>(nval_warp) * kTilePix;
+      }
       float t_re[R], t_im[R];
       double e_re[R], e_im[R];
 #pragma unroll
@@ -192,17 +232,7 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
-            if (FP64) {
-              double sn, cs;
-              sincos_turns_fp64(t, sn, cs);
-              e_re[r] = fma(static_cast<double>(I), cs, e_re[r]);
-              e_im[r] = fma(-static_cast<double>(I), sn, e_im[r]);
-            } else {
-              float sn, cs;
-              __sincosf(turn_angle(t), &sn, &cs);
-              t_re[r] = fmaf(I, cs, t_re[r]);
-              t_im[r] = fmaf(-I, sn, t_im[r]);
-            }
+            fwd_term<FP64>(t, I, t_re[r], t_im[r], e_re[r], e_im[r]);
           }
         }
       } else {
@@ -210,23 +240,20 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           if ((st[r] & 3) == 0) continue;
-          double4 q0, q1, q2;
-          mixed_rows(rf[r], st[r], p.occ, q0, q1, q2);
-          for (int j = 0; j < kTilePix; ++j) {
-            const double4 q = tp[j];
-            const bool vis = visible_rows(q0, q1, q2, q.x, q.y, q.z);
-            const float Iv = vis ? sky_of(q) : 0.f;
-            const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
-            if (FP64) {
-              double sn, cs;
-              sincos_turns_fp64(t, sn, cs);
-              e_re[r] = fma(static_cast<double>(Iv), cs, e_re[r]);
-              e_im[r] = fma(-static_cast<double>(Iv), sn, e_im[r]);
-            } else {
-              float sn, cs;
-              __sincosf(turn_angle(t), &sn, &cs);
-              t_re[r] = fmaf(Iv, cs, t_re[r]);
-              t_im[r] = fmaf(-Iv, sn, t_im[r]);
+          if (st[r] == 2) {
+            for (int j = 0; j < kTilePix; ++j) {
+              const double4 q = tp[j];
+              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
+              fwd_term<FP64>(t, sky_of(q), t_re[r], t_im[r], e_re[r], e_im[r]);
+            }
+          } else {
+            double4 q0, q1, q2;
+            mixed_rows(s_refs[r][tid], st[r], p.occ, q0, q1, q2);
+            for (int j = 0; j < kTilePix; ++j) {
+              const double4 q = tp[j];
+              const float Iv = visible_rows(q0, q1, q2, q.x, q.y, q.z) ? sky_of(q) : 0.f;
+              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
+              fwd_term<FP64>(t, Iv, t_re[r], t_im[r], e_re[r], e_im[r]);
             }
           }
         }
@@ -250,7 +277,10 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
     }
   }
 
-  if (p.counter && (tid & 31) == 0 && evaluated) atomicAdd(p.counter, evaluated);
+  if (p.counter && (tid & 31) == 0) {
+    if (evaluated) atomicAdd(p.counter, evaluated);
+    if (mixed_terms) atomicAdd(p.counter + 2, mixed_terms);
+  }
   double2 *out = p.part + static_cast<long long>(blockIdx.y) * p.K;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -290,9 +320,41 @@ __global__ void k_reduce_fwd(long long K, int nchunk, const double2 *part, float
 // ======================================================================
 // adjoint
 // ======================================================================
+template <int P, bool MIXED, bool FP64>
+__device__ __forceinline__ void adj_sample(const double4 &u, double m, const float2 &a,
+                                           const double (&sx)[P], const double (&sy)[P],
+                                           const double (&sz)[P], const double4 &q0,
+                                           const double4 &q1, const double4 &q2, float (&acc)[P],
+                                           double (&dacc)[P]) {
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const double t = fma(u.z, sz[q], fma(u.y, sy[q], fma(u.x, sx[q], m)));
+    bool vis = true;
+    if (MIXED) vis = visible_rows(q0, q1, q2, sx[q], sy[q], sz[q]);
+    if (FP64) {
+      double sn, cs;
+      sincos_turns_fp64(t, sn, cs);
+      const double c = fma(static_cast<double>(a.x), cs, -static_cast<double>(a.y) * sn);
+      dacc[q] += vis ? c : 0.0;
+    } else {
+      float sn, cs;
+      sfu_sincos(turn_angle(t), sn, cs);
+      if (MIXED) {
+        const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
+        acc[q] = fmaf(ar, cs, acc[q]);
+        acc[q] = fmaf(-ai, sn, acc[q]);
+      } else {
+        acc[q] = fmaf(a.x, cs, acc[q]);
+        acc[q] = fmaf(-a.y, sn, acc[q]);
+      }
+    }
+  }
+}
+
 template <int NT, int P, bool MASKED, bool FP64>
 __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p) {
-  static_assert(P * 32 == kTilePix, "one warp covers one pixel tile");
+  static_assert(P == 4 || P == 8, "a warp covers one or two pixel tiles");
+  constexpr int kWarpPix = 32 * P;
   __shared__ __align__(128) double4 s_samp[2][kSampTile];
   __shared__ __align__(16) float2 s_coef[2][kSampTile];
   __shared__ __align__(16) int4 s_refs[MASKED ? 2 : 1][MASKED ? kSampTile : 1];
@@ -301,8 +363,8 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int kWarps = NT / 32;
-  const long long tile = static_cast<long long>(blockIdx.x) * kWarps + warp;  // pixel tile of this warp
-  const long long pbase = tile * kTilePix;
+  const long long wtile = static_cast<long long>(blockIdx.x) * kWarps + warp;
+  const long long pbase = wtile * kWarpPix;
   const bool tile_ok = pbase < p.Jpad;
 
   double sx[P], sy[P], sz[P];
@@ -312,7 +374,11 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
     const double4 v = tile_ok ? p.pix[j] : make_double4(0, 0, 1, 0);
     sx[q] = v.x; sy[q] = v.y; sz[q] = v.z;
   }
-  const double4 cone = (MASKED && tile_ok) ? p.cones[tile] : make_double4(0, 0, 1, 4.0);
+  double4 cone0 = make_double4(0, 0, 1, 4.0), cone1 = cone0;
+  if (MASKED && tile_ok) {
+    cone0 = p.cones[pbase / kTilePix];
+    if (P == 8) cone1 = p.cones[pbase / kTilePix + 1];
+  }
 
   float ks[P], kc[P];
   double dacc[P];
@@ -344,7 +410,8 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
   __syncthreads();
   if (tid == 0 && ntile > 0) issue(0, 0);
 
-  unsigned long long evaluated = 0;
+  unsigned long long evaluated = 0, mixed_terms = 0;
+  const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
   for (int it = 0; it < ntile; ++it) {
     const int buf = it & 1;
     const uint32_t par = (it >> 1) & 1;
@@ -358,14 +425,20 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
     const double4 *sp = s_samp[buf];
     const float2 *cp = s_coef[buf];
     for (int g = 0; g < n; g += 32) {
-      // lane l classifies sample g+l against this warp's tile
-      int st = 2;
+      // lane l classifies sample g+l against this warp's pixels
+      const int gn = min(32, n - g);
+      int st = (lane < gn) ? 2 : 0;
       if (MASKED) {
         st = 0;
-        if (g + lane < n && tile_ok) st = sample_state(s_refs[buf][g + lane], cone, p.occ);
+        if (lane < gn && tile_ok) {
+          const int4 rf = s_refs[buf][g + lane];
+          st = (P == 8) ? sample_state2(rf, cone0, cone1, p.occ) : sample_state(rf, cone0, p.occ);
+        }
       }
-      const int gn = min(32, n - g);
-      unsigned long long ev = 0;
+      const unsigned live = __ballot_sync(0xffffffffu, (st & 3) != 0);
+      const unsigned mix = __ballot_sync(0xffffffffu, (st & 3) == 1);
+      evaluated += static_cast<unsigned long long>(__popc(live)) * kWarpPix;
+      mixed_terms += static_cast<unsigned long long>(__popc(mix)) * kWarpPix;
       float t_acc[P];
       double e_acc[P];
 #pragma unroll
@@ -373,31 +446,16 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
       for (int i = 0; i < gn; ++i) {
         const int sst = MASKED ? __shfl_sync(0xffffffffu, st, i) : 2;
         if ((sst & 3) == 0) continue;
-        ev += kTilePix;
         const double4 u = sp[g + i];
         const float2 a = cp[g + i];
         const double uoff = p.use_off ? u.w : 0.0;
         const double m = FP64 ? uoff : kMagic + uoff;
-        const bool mixed = MASKED && (sst & 3) == 1;
-        double4 q0, q1, q2;
-        if (mixed) mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-          bool vis = true;
-          if (mixed) vis = visible_rows(q0, q1, q2, sx[q], sy[q], sz[q]);
-          const double t = fma(u.z, sz[q], fma(u.y, sy[q], fma(u.x, sx[q], m)));
-          if (FP64) {
-            double sn, cs;
-            sincos_turns_fp64(t, sn, cs);
-            const double c = fma(static_cast<double>(a.x), cs, -static_cast<double>(a.y) * sn);
-            e_acc[q] += vis ? c : 0.0;
-          } else {
-            float sn, cs;
-            __sincosf(turn_angle(t), &sn, &cs);
-            const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
-            t_acc[q] = fmaf(ar, cs, t_acc[q]);
-            t_acc[q] = fmaf(-ai, sn, t_acc[q]);
-          }
+        if (!MASKED || (sst & 3) == 2) {
+          adj_sample<P, false, FP64>(u, m, a, sx, sy, sz, pass, pass, pass, t_acc, e_acc);
+        } else {
+          double4 q0, q1, q2;
+          mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
+          adj_sample<P, true, FP64>(u, m, a, sx, sy, sz, q0, q1, q2, t_acc, e_acc);
         }
       }
 #pragma unroll
@@ -405,7 +463,6 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
         if (FP64) dacc[q] += e_acc[q];
         else kahan_add(ks[q], kc[q], t_acc[q]);
       }
-      if (lane == 0) evaluated += ev;
     }
     __syncthreads();
     if (s_abort) {
@@ -414,7 +471,10 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
     }
   }
 
-  if (p.counter && lane == 0 && evaluated && tile_ok) atomicAdd(p.counter, evaluated);
+  if (p.counter && lane == 0 && tile_ok) {
+    if (evaluated) atomicAdd(p.counter, evaluated);
+    if (mixed_terms) atomicAdd(p.counter + 2, mixed_terms);
+  }
   if (!tile_ok) return;
   double *out = p.part + static_cast<long long>(blockIdx.y) * p.Jpad;
 #pragma unroll
@@ -442,7 +502,6 @@ __global__ void k_reduce_adj(long long J, long long Jpad, int nchunk, const doub
 // ---------------------------------------------------------------- launchers
 namespace viss {
 
-// Launch shapes (template instances); the plan's tuner picks among these.
 constexpr int kFwdNT = 256;
 constexpr int kAdjNT = 256;
 
@@ -455,25 +514,15 @@ static cudaError_t fwd_inst(const FwdParams &p, int nchunk, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int R>
-static cudaError_t fwd_dispatch(const FwdParams &p, int nchunk, bool masked, bool fp64,
-                                cudaStream_t st) {
-  if (fp64) return masked ? fwd_inst<R, true, true>(p, nchunk, st) : fwd_inst<R, false, true>(p, nchunk, st);
-  return masked ? fwd_inst<R, true, false>(p, nchunk, st) : fwd_inst<R, false, false>(p, nchunk, st);
-}
-
 cudaError_t launch_forward(const FwdParams &p, int R, int nchunk, bool masked, bool fp64,
                            cudaStream_t st) {
   if (p.K <= 0 || p.ntiles <= 0) return cudaSuccess;
-  if (fp64) return fwd_dispatch<2>(p, nchunk, masked, true, st);
-  switch (R) {
-    case 2: return fwd_dispatch<2>(p, nchunk, masked, false, st);
-    case 8: return fwd_dispatch<8>(p, nchunk, masked, false, st);
-    default: return fwd_dispatch<4>(p, nchunk, masked, false, st);
-  }
+  if (fp64) return masked ? fwd_inst<2, true, true>(p, nchunk, st) : fwd_inst<2, false, true>(p, nchunk, st);
+  if (R == 2) return masked ? fwd_inst<2, true, false>(p, nchunk, st) : fwd_inst<2, false, false>(p, nchunk, st);
+  return masked ? fwd_inst<4, true, false>(p, nchunk, st) : fwd_inst<4, false, false>(p, nchunk, st);
 }
 
-int forward_samples_per_block(int R, bool fp64) { return kFwdNT * (fp64 ? 2 : R); }
+int forward_samples_per_block(int R, bool fp64) { return kFwdNT * (fp64 ? 2 : (R == 2 ? 2 : 4)); }
 
 cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
                               cudaStream_t st) {
@@ -482,20 +531,23 @@ cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, floa
   return cudaGetLastError();
 }
 
-template <bool M, bool F>
+int adjoint_pixels_per_block(int P, bool fp64) { return (kAdjNT / 32) * 32 * (fp64 ? 4 : P); }
+
+template <int P, bool M, bool F>
 static cudaError_t adj_inst(const AdjParams &p, int nchunk, cudaStream_t st) {
-  const long long pix_per_cta = static_cast<long long>(kAdjNT / 32) * kTilePix;
+  const long long pix_per_cta = static_cast<long long>(kAdjNT / 32) * 32 * P;
   const unsigned gx = static_cast<unsigned>((p.Jpad + pix_per_cta - 1) / pix_per_cta);
   dim3 grid(gx, nchunk);
-  k_adjoint<kAdjNT, kTilePix / 32, M, F><<<grid, kAdjNT, 0, st>>>(p);
+  k_adjoint<kAdjNT, P, M, F><<<grid, kAdjNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint(const AdjParams &p, int nchunk, bool masked, bool fp64,
+cudaError_t launch_adjoint(const AdjParams &p, int P, int nchunk, bool masked, bool fp64,
                            cudaStream_t st) {
   if (p.K <= 0 || p.Jpad <= 0) return cudaSuccess;
-  if (fp64) return masked ? adj_inst<true, true>(p, nchunk, st) : adj_inst<false, true>(p, nchunk, st);
-  return masked ? adj_inst<true, false>(p, nchunk, st) : adj_inst<false, false>(p, nchunk, st);
+  if (fp64) return masked ? adj_inst<4, true, true>(p, nchunk, st) : adj_inst<4, false, true>(p, nchunk, st);
+  if (P == 8) return masked ? adj_inst<8, true, false>(p, nchunk, st) : adj_inst<8, false, false>(p, nchunk, st);
+  return masked ? adj_inst<4, true, false>(p, nchunk, st) : adj_inst<4, false, false>(p, nchunk, st);
 }
 
 cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,

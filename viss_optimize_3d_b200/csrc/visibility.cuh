@@ -18,7 +18,7 @@ struct FwdParams {
   int ntiles;
   int tiles_per_chunk;
   double2 *part;                // [nchunk][K]
-  unsigned long long *counter;  // exponentials evaluated
+  unsigned long long *counter;  // [0] exponentials evaluated, [2] of them in mixed tiles
   int *err;
   int use_off;                  // add the per-sample offset (.w) to the phase
 };
@@ -44,8 +44,9 @@ cudaError_t launch_forward(const FwdParams &p, int R, int nchunk, bool masked, b
 int forward_samples_per_block(int R, bool fp64);
 cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
                               cudaStream_t st);
-cudaError_t launch_adjoint(const AdjParams &p, int nchunk, bool masked, bool fp64,
+cudaError_t launch_adjoint(const AdjParams &p, int P, int nchunk, bool masked, bool fp64,
                            cudaStream_t st);
+int adjoint_pixels_per_block(int P, bool fp64);
 cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
                               const int *perm, float scale, float *img, int acc, cudaStream_t st);
 

@@ -88,12 +88,21 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
 // ------------------------------------------------------------- phase helpers
 // Reduced angle (radians, [-pi, pi)) from t = kMagic + phase: the low 23
 // mantissa bits of t are frac(phase + 1/2) in units of 2^-23 turn; placed
-// under the exponent of 1.0f they give f in [1, 2), and 2 pi f - 3 pi is the
-// phase reduced mod one turn.
+// under the exponent of 1.0f (one LOP3: (lo & 0x7fffff) | 0x3f800000) they
+// give f in [1, 2), and 2 pi f - 3 pi is the phase reduced mod one turn.
 __device__ __forceinline__ float turn_angle(double t) {
   const uint32_t lo = static_cast<uint32_t>(__double2loint(t));
-  const float f = __uint_as_float((lo & 0x007fffffu) | 0x3f800000u);
-  return fmaf(f, 6.28318530717958648f, -9.42477796076937972f);
+  uint32_t bits;
+  asm("lop3.b32 %0, %1, %2, %3, 0xEA;" : "=r"(bits) : "r"(lo), "r"(0x007fffffu), "r"(0x3f800000u));
+  return fmaf(__uint_as_float(bits), 6.28318530717958648f, -9.42477796076937972f);
+}
+
+// SFU sine and cosine of an angle in [-pi, pi) (flush-to-zero variants: the
+// reduced angle is never subnormal in a way that matters, and .ftz avoids the
+// subnormal fix-up instructions).
+__device__ __forceinline__ void sfu_sincos(float a, float &s, float &c) {
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(a));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(a));
 }
 
 // Exact-op-order dot product used by the occultation predicate (the oracle
