@@ -141,6 +141,24 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    # launch-shape sweep (recorded) and the plan's own tuner (chooses)
+    V0 = g.plan.forward(g.sky)
+    gs0, _c0, dcf0 = api.dcf(g.bll, g.nr, multiplicity=2)
+    coef0 = api.scale_coef(api.weights(g.w, g.bll, gs0, dcf0, g.nr)[1], V0)
+    sweep = {"forward_ms": [], "adjoint_ms": []}
+    for shape in range(4):
+        g.plan.set_shapes(shape, shape)
+        for key, fn in (("forward_ms", lambda: g.plan.forward(g.sky)),
+                        ("adjoint_ms", lambda: g.plan.adjoint(coef0, scale=2.0, mask=cfg.imaging_mask))):
+            fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sweep[key].append(round(e0.elapsed_time(e1), 3))
+    shapes = g.plan.tune(g.sky, coef0, mask=cfg.imaging_mask)
+    torch.cuda.synchronize()
     fwd_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
     adj_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -269,6 +287,9 @@ def run_ours(args, rank, world, local_rank):
         "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_mixed": round(mx_f / tot, 4),
                     "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_mixed": round(mx_a / tot, 4)},
         "gpu_launches": 10 * args.steps,
+        "tuning": {"chosen": {"forward": shapes[0], "adjoint": shapes[1]},
+                   "forward_shapes": "(samples/thread, CTAs/SM) = (4,2) (4,3) (2,3) (2,4)",
+                   "adjoint_shapes": "(pixels/lane, CTAs/SM) = (8,2) (8,3) (4,3) (4,4)", **sweep},
         "clocks": clk,
     }
     if args.cpu_baseline:

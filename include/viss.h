@@ -133,6 +133,19 @@ int viss_forward(viss_plan *plan, const float *sky, float *V, int flags, void *s
 int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, int flags,
                  void *stream);
 
+/* Autotuner: times every launch shape of the forward and adjoint kernels on
+ * this plan's problem (CUDA events on `stream`, one warm-up and one timed
+ * launch each) and keeps the fastest for later calls.  sky (J FP32) and coef
+ * (K complex64) are representative inputs; V_scratch (K complex64) and
+ * img_scratch (J FP32) receive throw-away outputs.  Synchronous.  The chosen
+ * shape indices are returned through fwd_shape / adj_shape (may be NULL).
+ * No counterpart in the reference (it launches one fixed shape from
+ * cudaOccupancyMaxPotentialBlockSize, vissgen3d_blockage.cu:412-413). */
+int viss_plan_tune(viss_plan *plan, const float *sky, const float *coef, float *V_scratch,
+                   float *img_scratch, int flags, int *fwd_shape, int *adj_shape, void *stream);
+/* Sets the launch shapes directly (indices 0..3 each). */
+int viss_plan_set_shapes(viss_plan *plan, int fwd_shape, int adj_shape);
+
 /* Terms evaluated by the last viss_forward / viss_adjoint on this plan
  * (visible-or-mixed pairs actually exponentiated) and the total K*J, read
  * back from the device (synchronises the plan's last stream). */

@@ -202,6 +202,25 @@ class Plan:
         check(lib.viss_plan_last_counts(self._h, C.byref(ev), C.byref(tot)), "viss_plan_last_counts")
         return ev.value, tot.value
 
+    def tune(self, sky, coef=None, mask: bool = True, use_offset: bool = True):
+        """Time every launch shape on this problem and keep the fastest
+        (synchronous); returns (forward shape, adjoint shape)."""
+        sky = _cuda(sky, torch.float32, self.device)
+        if coef is None:
+            coef = torch.ones(self.K, dtype=torch.complex64, device=self.device)
+        coef = _cuda(coef, torch.complex64, self.device)
+        V = torch.empty(self.K, dtype=torch.complex64, device=self.device)
+        img = torch.empty(self.J, dtype=torch.float32, device=self.device)
+        fs, as_ = C.c_int(), C.c_int()
+        check(lib.viss_plan_tune(self._h, _p(sky), _p(coef), _p(V), _p(img),
+                                 self._flags(False, mask, use_offset), C.byref(fs), C.byref(as_),
+                                 _stream(sky)), "viss_plan_tune")
+        return fs.value, as_.value
+
+    def set_shapes(self, fwd_shape: int, adj_shape: int):
+        check(lib.viss_plan_set_shapes(self._h, int(fwd_shape), int(adj_shape)),
+              "viss_plan_set_shapes")
+
     def last_stats(self):
         """(evaluated, evaluated in mixed tiles, K*J) of the last call (syncs)."""
         ev, mx, tot = C.c_int64(), C.c_int64(), C.c_int64()

@@ -122,27 +122,27 @@ struct viss_plan {
   long long last_total = 0;
   cudaStream_t last_stream = nullptr;
   // launch shape
-  int fwd_R = 4;
-  int adj_P = 8;
+  int fwd_shape = 0;   // index into viss::kFwdShapes (viss_plan_tune picks it)
+  int adj_shape = 0;   // index into viss::kAdjShapes
   int fwd_waves = 16;
   int adj_waves = 16;
 };
 
 namespace {
 
-int fwd_chunks(const viss_plan *p, int R, bool fp64) {
-  const long long per = viss::forward_samples_per_block(R, fp64);
+int fwd_chunks(const viss_plan *p, int shape, bool fp64) {
+  const long long per = viss::forward_samples_per_block(shape, fp64);
   const long long blocks = (p->K + per - 1) / per;
-  const long long slots = static_cast<long long>(p->nsm) * (fp64 ? 1 : 2);
+  const long long slots = static_cast<long long>(p->nsm) * viss::forward_ctas_per_sm(shape, fp64);
   long long c = (static_cast<long long>(p->fwd_waves) * slots + blocks - 1) / blocks;
   c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 2)));
   return static_cast<int>(c);
 }
 
-int adj_chunks(const viss_plan *p, bool fp64, int *samples_per_chunk) {
-  const long long per = viss::adjoint_pixels_per_block(p->adj_P, fp64);  // pixels per CTA
+int adj_chunks(const viss_plan *p, int shape, bool fp64, int *samples_per_chunk) {
+  const long long per = viss::adjoint_pixels_per_block(shape, fp64);  // pixels per CTA
   const long long blocks = (p->Jpad + per - 1) / per;
-  const long long slots = static_cast<long long>(p->nsm) * (fp64 ? 1 : 2);
+  const long long slots = static_cast<long long>(p->nsm) * viss::adjoint_ctas_per_sm(shape, fp64);
   long long c = (static_cast<long long>(p->adj_waves) * slots + blocks - 1) / blocks;
   const long long max_c = std::max<long long>(1, (p->K + 255) / 256);
   c = std::max<long long>(1, std::min(c, max_c));
@@ -371,16 +371,11 @@ static int workspace(viss_plan *p, size_t bytes) {
   return ensure(p->part, p->part_cap, bytes, "partial-sum workspace");
 }
 
-int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stream) {
-  if (!p || !sky || !V) return fail(VISS_ERR_ARG, "viss_forward: bad arguments");
-  if (p->J <= 0 || p->K <= 0) return fail(VISS_ERR_STATE, "viss_forward: pixels or samples not set");
+static int forward_impl(viss_plan *p, const float *sky, float *V, int flags, cudaStream_t st,
+                        int shape) {
   const bool fp64 = (flags & VISS_FP64) != 0;
   const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
-  if (!fp64 && !(p->max_turns < viss::kMaxTurns))
-    return fail(VISS_ERR_ARG, "viss_forward: |u|+|v|+|w|+|off| exceeds 2^28 turns; use VISS_FP64");
-  const cudaStream_t st = as_stream(stream);
-  const int R = fp64 ? 2 : p->fwd_R;
-  const int nchunk = fwd_chunks(p, R, fp64);
+  const int nchunk = fwd_chunks(p, shape, fp64);
   if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * p->K)) return s;
   VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, st),
             "viss_forward: sky");
@@ -399,7 +394,7 @@ int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stre
   fp.counter = p->dev_words;
   fp.err = reinterpret_cast<int *>(p->dev_words + 1);
   fp.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
-  VISS_CUDA(viss::launch_forward(fp, R, real_chunks, masked, fp64, st), "viss_forward: kernel");
+  VISS_CUDA(viss::launch_forward(fp, shape, real_chunks, masked, fp64, st), "viss_forward: kernel");
   VISS_CUDA(viss::launch_reduce_fwd(p->K, real_chunks, fp.part, reinterpret_cast<float2 *>(V),
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_forward: reduce");
@@ -408,16 +403,26 @@ int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stre
   return VISS_OK;
 }
 
-int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int flags, void *stream) {
-  if (!p || !coef || !image) return fail(VISS_ERR_ARG, "viss_adjoint: bad arguments");
-  if (p->J <= 0 || p->K <= 0) return fail(VISS_ERR_STATE, "viss_adjoint: pixels or samples not set");
+static int check_call(viss_plan *p, const void *in, const void *out, int flags, const char *who) {
+  if (!p || !in || !out) return fail(VISS_ERR_ARG, std::string(who) + ": bad arguments");
+  if (p->J <= 0 || p->K <= 0)
+    return fail(VISS_ERR_STATE, std::string(who) + ": pixels or samples not set");
+  if (!(flags & VISS_FP64) && !(p->max_turns < viss::kMaxTurns))
+    return fail(VISS_ERR_ARG, std::string(who) + ": |u|+|v|+|w|+|off| exceeds 2^28 turns; use VISS_FP64");
+  return VISS_OK;
+}
+
+int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stream) {
+  if (int s = check_call(p, sky, V, flags, "viss_forward")) return s;
+  return forward_impl(p, sky, V, flags, as_stream(stream), p->fwd_shape);
+}
+
+static int adjoint_impl(viss_plan *p, const float *coef, float *image, float scale, int flags,
+                        cudaStream_t st, int shape) {
   const bool fp64 = (flags & VISS_FP64) != 0;
   const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
-  if (!fp64 && !(p->max_turns < viss::kMaxTurns))
-    return fail(VISS_ERR_ARG, "viss_adjoint: |u|+|v|+|w|+|off| exceeds 2^28 turns; use VISS_FP64");
-  const cudaStream_t st = as_stream(stream);
   int spc = 0;
-  const int nchunk = adj_chunks(p, fp64, &spc);
+  const int nchunk = adj_chunks(p, shape, fp64, &spc);
   if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->Jpad)) return s;
   VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
             "viss_adjoint: coef");
@@ -436,12 +441,72 @@ int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int
   ap.counter = p->dev_words;
   ap.err = reinterpret_cast<int *>(p->dev_words + 1);
   ap.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
-  VISS_CUDA(viss::launch_adjoint(ap, p->adj_P, nchunk, masked, fp64, st), "viss_adjoint: kernel");
+  VISS_CUDA(viss::launch_adjoint(ap, shape, nchunk, masked, fp64, st), "viss_adjoint: kernel");
   VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, ap.part, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_adjoint: reduce");
   p->last_total = p->K * p->J;
   p->last_stream = st;
+  return VISS_OK;
+}
+
+int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int flags, void *stream) {
+  if (int s = check_call(p, coef, image, flags, "viss_adjoint")) return s;
+  return adjoint_impl(p, coef, image, scale, flags, as_stream(stream), p->adj_shape);
+}
+
+// Times every launch shape of both kernels on this plan's problem (one warm-up
+// and one timed launch each, CUDA events on `stream`) and keeps the fastest.
+// Synchronous; call before capturing the plan's calls in a CUDA graph.
+int viss_plan_tune(viss_plan *p, const float *sky, const float *coef, float *V_scratch,
+                   float *img_scratch, int flags, int *fwd_shape, int *adj_shape, void *stream) {
+  if (int s = check_call(p, sky, V_scratch, flags, "viss_plan_tune")) return s;
+  if (!coef || !img_scratch) return fail(VISS_ERR_ARG, "viss_plan_tune: bad arguments");
+  if (flags & VISS_FP64) return fail(VISS_ERR_ARG, "viss_plan_tune: tunes the split path only");
+  const cudaStream_t st = as_stream(stream);
+  cudaEvent_t e0, e1;
+  VISS_CUDA(cudaEventCreate(&e0), "viss_plan_tune");
+  VISS_CUDA(cudaEventCreate(&e1), "viss_plan_tune");
+  float best_f = 1e30f, best_a = 1e30f;
+  int bf = p->fwd_shape, ba = p->adj_shape, status = VISS_OK;
+  for (int s = 0; s < viss::kNumFwdShapes && status == VISS_OK; ++s) {
+    status = forward_impl(p, sky, V_scratch, flags, st, s);
+    if (status) break;
+    cudaEventRecord(e0, st);
+    status = forward_impl(p, sky, V_scratch, flags, st, s);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { status = cuda_fail(cudaGetLastError(), "viss_plan_tune"); break; }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_f) { best_f = ms; bf = s; }
+  }
+  for (int s = 0; s < viss::kNumAdjShapes && status == VISS_OK; ++s) {
+    status = adjoint_impl(p, coef, img_scratch, 1.0f, flags, st, s);
+    if (status) break;
+    cudaEventRecord(e0, st);
+    status = adjoint_impl(p, coef, img_scratch, 1.0f, flags, st, s);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { status = cuda_fail(cudaGetLastError(), "viss_plan_tune"); break; }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_a) { best_a = ms; ba = s; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status) return status;
+  p->fwd_shape = bf;
+  p->adj_shape = ba;
+  if (fwd_shape) *fwd_shape = bf;
+  if (adj_shape) *adj_shape = ba;
+  return VISS_OK;
+}
+
+int viss_plan_set_shapes(viss_plan *p, int fwd_shape, int adj_shape) {
+  if (!p || fwd_shape < 0 || fwd_shape >= viss::kNumFwdShapes || adj_shape < 0 ||
+      adj_shape >= viss::kNumAdjShapes)
+    return fail(VISS_ERR_ARG, "viss_plan_set_shapes: bad arguments");
+  p->fwd_shape = fwd_shape;
+  p->adj_shape = adj_shape;
   return VISS_OK;
 }
 

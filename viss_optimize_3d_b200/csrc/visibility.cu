@@ -129,10 +129,13 @@ __device__ __forceinline__ void fwd_term(double t, float I, float &re, float &im
 // ======================================================================
 // forward
 // ======================================================================
-template <int NT, int R, bool MASKED, bool FP64>
-__global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p) {
+template <int NT, int R, int MINB, bool MASKED, bool FP64>
+__global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   __shared__ __align__(128) double4 s_pix[2][kTilePix];
   __shared__ __align__(16) int4 s_refs[MASKED ? R : 1][MASKED ? NT : 1];
+  // Kahan (sum, comp) of re and im per sample, kept in shared memory (touched
+  // once per tile) so the registers hold only what the inner loop needs
+  __shared__ float s_kahan[FP64 ? 1 : 4][FP64 ? 1 : R][FP64 ? 1 : NT];
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ int s_abort;
 
@@ -155,13 +158,12 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
 #pragma unroll
   for (int r = 0; r < R; ++r) nval_warp += __popc(__ballot_sync(0xffffffffu, kval[r]));
 
-  // accumulators: split -> Kahan FP32 (sum, comp); FP64 -> plain double
-  float ks_re[R], kc_re[R], ks_im[R], kc_im[R];
+  // accumulators: split -> Kahan FP32 in shared memory; FP64 -> plain double
   double d_re[R], d_im[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    ks_re[r] = kc_re[r] = ks_im[r] = kc_im[r] = 0.f;
     d_re[r] = d_im[r] = 0.0;
+    if (!FP64) s_kahan[0][r][tid] = s_kahan[1][r][tid] = s_kahan[2][r][tid] = s_kahan[3][r][tid] = 0.f;
   }
 
   const int t0 = blockIdx.y * p.tiles_per_chunk;
@@ -264,8 +266,12 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
           d_re[r] += e_re[r];
           d_im[r] += e_im[r];
         } else {
-          kahan_add(ks_re[r], kc_re[r], t_re[r]);
-          kahan_add(ks_im[r], kc_im[r], t_im[r]);
+          float s0 = s_kahan[0][r][tid], c0 = s_kahan[1][r][tid];
+          float s1 = s_kahan[2][r][tid], c1 = s_kahan[3][r][tid];
+          kahan_add(s0, c0, t_re[r]);
+          kahan_add(s1, c1, t_im[r]);
+          s_kahan[0][r][tid] = s0; s_kahan[1][r][tid] = c0;
+          s_kahan[2][r][tid] = s1; s_kahan[3][r][tid] = c1;
         }
       }
     }
@@ -291,8 +297,8 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_forward(const FwdParams p)
       v.x = d_re[r];
       v.y = d_im[r];
     } else {
-      v.x = static_cast<double>(ks_re[r]) - static_cast<double>(kc_re[r]);
-      v.y = static_cast<double>(ks_im[r]) - static_cast<double>(kc_im[r]);
+      v.x = static_cast<double>(s_kahan[0][r][tid]) - static_cast<double>(s_kahan[1][r][tid]);
+      v.y = static_cast<double>(s_kahan[2][r][tid]) - static_cast<double>(s_kahan[3][r][tid]);
     }
     out[k] = v;
   }
@@ -351,10 +357,11 @@ __device__ __forceinline__ void adj_sample(const double4 &u, double m, const flo
   }
 }
 
-template <int NT, int P, bool MASKED, bool FP64>
-__global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p) {
+template <int NT, int P, int MINB, bool MASKED, bool FP64>
+__global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   static_assert(P == 4 || P == 8, "a warp covers one or two pixel tiles");
   constexpr int kWarpPix = 32 * P;
+  __shared__ float s_kahan[FP64 ? 1 : 2][FP64 ? 1 : P][FP64 ? 1 : NT];  // (sum, comp) per pixel
   __shared__ __align__(128) double4 s_samp[2][kSampTile];
   __shared__ __align__(16) float2 s_coef[2][kSampTile];
   __shared__ __align__(16) int4 s_refs[MASKED ? 2 : 1][MASKED ? kSampTile : 1];
@@ -380,10 +387,12 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
     if (P == 8) cone1 = p.cones[pbase / kTilePix + 1];
   }
 
-  float ks[P], kc[P];
   double dacc[P];
 #pragma unroll
-  for (int q = 0; q < P; ++q) { ks[q] = kc[q] = 0.f; dacc[q] = 0.0; }
+  for (int q = 0; q < P; ++q) {
+    dacc[q] = 0.0;
+    if (!FP64) s_kahan[0][q][tid] = s_kahan[1][q][tid] = 0.f;
+  }
 
   const long long k0 = static_cast<long long>(blockIdx.y) * p.samples_per_chunk;
   const long long k1 = min(k0 + p.samples_per_chunk, p.K);
@@ -424,6 +433,12 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
     const int n = static_cast<int>(min(static_cast<long long>(kSampTile), k1 - kk));
     const double4 *sp = s_samp[buf];
     const float2 *cp = s_coef[buf];
+    // plain FP32 sums over this staged tile (<= 128 samples per pixel), then
+    // one Kahan fold into shared memory
+    float t_acc[P];
+    double e_acc[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) { t_acc[q] = 0.f; e_acc[q] = 0.0; }
     for (int g = 0; g < n; g += 32) {
       // lane l classifies sample g+l against this warp's pixels
       const int gn = min(32, n - g);
@@ -436,32 +451,40 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
         }
       }
       const unsigned live = __ballot_sync(0xffffffffu, (st & 3) != 0);
-      const unsigned mix = __ballot_sync(0xffffffffu, (st & 3) == 1);
+      const unsigned mixm = __ballot_sync(0xffffffffu, (st & 3) == 1);
       evaluated += static_cast<unsigned long long>(__popc(live)) * kWarpPix;
-      mixed_terms += static_cast<unsigned long long>(__popc(mix)) * kWarpPix;
-      float t_acc[P];
-      double e_acc[P];
-#pragma unroll
-      for (int q = 0; q < P; ++q) { t_acc[q] = 0.f; e_acc[q] = 0.0; }
-      for (int i = 0; i < gn; ++i) {
-        const int sst = MASKED ? __shfl_sync(0xffffffffu, st, i) : 2;
-        if ((sst & 3) == 0) continue;
+      mixed_terms += static_cast<unsigned long long>(__popc(mixm)) * kWarpPix;
+      // samples visible on every pixel of the warp: no test, uniform loop
+      for (unsigned fast = live & ~mixm; fast; fast &= fast - 1) {
+        const int i = __ffs(fast) - 1;
         const double4 u = sp[g + i];
         const float2 a = cp[g + i];
         const double uoff = p.use_off ? u.w : 0.0;
-        const double m = FP64 ? uoff : kMagic + uoff;
-        if (!MASKED || (sst & 3) == 2) {
-          adj_sample<P, false, FP64>(u, m, a, sx, sy, sz, pass, pass, pass, t_acc, e_acc);
-        } else {
-          double4 q0, q1, q2;
-          mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
-          adj_sample<P, true, FP64>(u, m, a, sx, sy, sz, q0, q1, q2, t_acc, e_acc);
-        }
+        adj_sample<P, false, FP64>(u, FP64 ? uoff : kMagic + uoff, a, sx, sy, sz, pass, pass,
+                                   pass, t_acc, e_acc);
       }
+      // samples that need the per-pixel occultation test
+      for (unsigned mb = mixm; mb; mb &= mb - 1) {
+        const int i = __ffs(mb) - 1;
+        const int sst = __shfl_sync(0xffffffffu, st, i);
+        const double4 u = sp[g + i];
+        const float2 a = cp[g + i];
+        const double uoff = p.use_off ? u.w : 0.0;
+        double4 q0, q1, q2;
+        mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
+        adj_sample<P, true, FP64>(u, FP64 ? uoff : kMagic + uoff, a, sx, sy, sz, q0, q1, q2,
+                                  t_acc, e_acc);
+      }
+    }
 #pragma unroll
-      for (int q = 0; q < P; ++q) {
-        if (FP64) dacc[q] += e_acc[q];
-        else kahan_add(ks[q], kc[q], t_acc[q]);
+    for (int q = 0; q < P; ++q) {
+      if (FP64) {
+        dacc[q] += e_acc[q];
+      } else {
+        float s = s_kahan[0][q][tid], c = s_kahan[1][q][tid];
+        kahan_add(s, c, t_acc[q]);
+        s_kahan[0][q][tid] = s;
+        s_kahan[1][q][tid] = c;
       }
     }
     __syncthreads();
@@ -480,7 +503,8 @@ __global__ void __launch_bounds__(NT, FP64 ? 1 : 2) k_adjoint(const AdjParams p)
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     const long long j = pbase + q * 32 + lane;
-    out[j] = FP64 ? dacc[q] : static_cast<double>(ks[q]) - static_cast<double>(kc[q]);
+    out[j] = FP64 ? dacc[q]
+                  : static_cast<double>(s_kahan[0][q][tid]) - static_cast<double>(s_kahan[1][q][tid]);
   }
 }
 
@@ -505,24 +529,46 @@ namespace viss {
 constexpr int kFwdNT = 256;
 constexpr int kAdjNT = 256;
 
-template <int R, bool M, bool F>
+// Launch shapes the plan's tuner chooses among: forward (samples per thread,
+// CTAs per SM) and adjoint (pixels per lane, CTAs per SM).
+const FwdShape kFwdShapes[kNumFwdShapes] = {{4, 2}, {4, 3}, {2, 3}, {2, 4}};
+const AdjShape kAdjShapes[kNumAdjShapes] = {{8, 2}, {8, 3}, {4, 3}, {4, 4}};
+
+template <int R, int MINB, bool M, bool F>
 static cudaError_t fwd_inst(const FwdParams &p, int nchunk, cudaStream_t st) {
   const long long per = static_cast<long long>(kFwdNT) * R;
   const unsigned gx = static_cast<unsigned>((p.K + per - 1) / per);
   dim3 grid(gx, nchunk);
-  k_forward<kFwdNT, R, M, F><<<grid, kFwdNT, 0, st>>>(p);
+  k_forward<kFwdNT, R, MINB, M, F><<<grid, kFwdNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward(const FwdParams &p, int R, int nchunk, bool masked, bool fp64,
-                           cudaStream_t st) {
-  if (p.K <= 0 || p.ntiles <= 0) return cudaSuccess;
-  if (fp64) return masked ? fwd_inst<2, true, true>(p, nchunk, st) : fwd_inst<2, false, true>(p, nchunk, st);
-  if (R == 2) return masked ? fwd_inst<2, true, false>(p, nchunk, st) : fwd_inst<2, false, false>(p, nchunk, st);
-  return masked ? fwd_inst<4, true, false>(p, nchunk, st) : fwd_inst<4, false, false>(p, nchunk, st);
+template <int R, int MINB>
+static cudaError_t fwd_m(const FwdParams &p, int nchunk, bool masked, cudaStream_t st) {
+  return masked ? fwd_inst<R, MINB, true, false>(p, nchunk, st)
+                : fwd_inst<R, MINB, false, false>(p, nchunk, st);
 }
 
-int forward_samples_per_block(int R, bool fp64) { return kFwdNT * (fp64 ? 2 : (R == 2 ? 2 : 4)); }
+cudaError_t launch_forward(const FwdParams &p, int shape, int nchunk, bool masked, bool fp64,
+                           cudaStream_t st) {
+  if (p.K <= 0 || p.ntiles <= 0) return cudaSuccess;
+  if (fp64) return masked ? fwd_inst<2, 1, true, true>(p, nchunk, st) : fwd_inst<2, 1, false, true>(p, nchunk, st);
+  switch (shape) {
+    case 1: return fwd_m<4, 3>(p, nchunk, masked, st);
+    case 2: return fwd_m<2, 3>(p, nchunk, masked, st);
+    case 3: return fwd_m<2, 4>(p, nchunk, masked, st);
+    default: return fwd_m<4, 2>(p, nchunk, masked, st);
+  }
+}
+
+int forward_samples_per_block(int shape, bool fp64) {
+  if (fp64) return kFwdNT * 2;
+  return kFwdNT * kFwdShapes[(shape >= 0 && shape < kNumFwdShapes) ? shape : 0].R;
+}
+int forward_ctas_per_sm(int shape, bool fp64) {
+  if (fp64) return 1;
+  return kFwdShapes[(shape >= 0 && shape < kNumFwdShapes) ? shape : 0].minb;
+}
 
 cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
                               cudaStream_t st) {
@@ -531,23 +577,40 @@ cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, floa
   return cudaGetLastError();
 }
 
-int adjoint_pixels_per_block(int P, bool fp64) { return (kAdjNT / 32) * 32 * (fp64 ? 4 : P); }
+int adjoint_pixels_per_block(int shape, bool fp64) {
+  if (fp64) return (kAdjNT / 32) * 32 * 4;
+  return (kAdjNT / 32) * 32 * kAdjShapes[(shape >= 0 && shape < kNumAdjShapes) ? shape : 0].P;
+}
+int adjoint_ctas_per_sm(int shape, bool fp64) {
+  if (fp64) return 1;
+  return kAdjShapes[(shape >= 0 && shape < kNumAdjShapes) ? shape : 0].minb;
+}
 
-template <int P, bool M, bool F>
+template <int P, int MINB, bool M, bool F>
 static cudaError_t adj_inst(const AdjParams &p, int nchunk, cudaStream_t st) {
   const long long pix_per_cta = static_cast<long long>(kAdjNT / 32) * 32 * P;
   const unsigned gx = static_cast<unsigned>((p.Jpad + pix_per_cta - 1) / pix_per_cta);
   dim3 grid(gx, nchunk);
-  k_adjoint<kAdjNT, P, M, F><<<grid, kAdjNT, 0, st>>>(p);
+  k_adjoint<kAdjNT, P, MINB, M, F><<<grid, kAdjNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint(const AdjParams &p, int P, int nchunk, bool masked, bool fp64,
+template <int P, int MINB>
+static cudaError_t adj_m(const AdjParams &p, int nchunk, bool masked, cudaStream_t st) {
+  return masked ? adj_inst<P, MINB, true, false>(p, nchunk, st)
+                : adj_inst<P, MINB, false, false>(p, nchunk, st);
+}
+
+cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool masked, bool fp64,
                            cudaStream_t st) {
   if (p.K <= 0 || p.Jpad <= 0) return cudaSuccess;
-  if (fp64) return masked ? adj_inst<4, true, true>(p, nchunk, st) : adj_inst<4, false, true>(p, nchunk, st);
-  if (P == 8) return masked ? adj_inst<8, true, false>(p, nchunk, st) : adj_inst<8, false, false>(p, nchunk, st);
-  return masked ? adj_inst<4, true, false>(p, nchunk, st) : adj_inst<4, false, false>(p, nchunk, st);
+  if (fp64) return masked ? adj_inst<4, 1, true, true>(p, nchunk, st) : adj_inst<4, 1, false, true>(p, nchunk, st);
+  switch (shape) {
+    case 1: return adj_m<8, 3>(p, nchunk, masked, st);
+    case 2: return adj_m<4, 3>(p, nchunk, masked, st);
+    case 3: return adj_m<4, 4>(p, nchunk, masked, st);
+    default: return adj_m<8, 2>(p, nchunk, masked, st);
+  }
 }
 
 cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,

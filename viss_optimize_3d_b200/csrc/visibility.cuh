@@ -39,14 +39,23 @@ struct AdjParams {
   int use_off;                  // add the per-sample offset (.w) to the phase
 };
 
-cudaError_t launch_forward(const FwdParams &p, int R, int nchunk, bool masked, bool fp64,
+struct FwdShape { int R, minb; };
+struct AdjShape { int P, minb; };
+constexpr int kNumFwdShapes = 4;
+constexpr int kNumAdjShapes = 4;
+extern const FwdShape kFwdShapes[kNumFwdShapes];
+extern const AdjShape kAdjShapes[kNumAdjShapes];
+
+cudaError_t launch_forward(const FwdParams &p, int shape, int nchunk, bool masked, bool fp64,
                            cudaStream_t st);
-int forward_samples_per_block(int R, bool fp64);
+int forward_samples_per_block(int shape, bool fp64);
+int forward_ctas_per_sm(int shape, bool fp64);
 cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
                               cudaStream_t st);
-cudaError_t launch_adjoint(const AdjParams &p, int P, int nchunk, bool masked, bool fp64,
+cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool masked, bool fp64,
                            cudaStream_t st);
-int adjoint_pixels_per_block(int P, bool fp64);
+int adjoint_pixels_per_block(int shape, bool fp64);
+int adjoint_ctas_per_sm(int shape, bool fp64);
 cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
                               const int *perm, float scale, float *img, int acc, cudaStream_t st);
 
