@@ -155,6 +155,22 @@ int viss_plan_last_counts(viss_plan *plan, int64_t *evaluated, int64_t *total);
  * staging wait that gave up. */
 int viss_plan_last_stats(viss_plan *plan, int64_t *evaluated, int64_t *mixed, int64_t *total);
 
+/* Forward visibilities without any device allocation, for callers that
+ * cannot call cudaMalloc (a host application that owns the device-memory
+ * budget through its own pool allocator, or a pipeline that must not
+ * allocate after start-up).  No counterpart in the reference.  Same result
+ * as viss_forward (split precision) for lmn (J x 3), sky (J), uvw (K x 3),
+ * off (K or NULL), refs (K x 3 or NULL) and occ (G x 4, 16-byte aligned);
+ * V is K complex64.  All intermediates live in one fixed 7.5 MiB __device__
+ * array that every GPU loading the library holds until the process exits.
+ * Limits: J <= 65536 pixels, K <= 32768 samples (else VISS_ERR_ARG).  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress)
+ * -- make it before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race.  Each call synchronises `stream` once. */
+int viss_forward_noalloc(int64_t J, const double *lmn, const float *sky, int64_t K,
+                         const double *uvw, const double *off, const int32_t *refs, int64_t G,
+                         const double *occ, float *V, void *stream);
+
 /* ----------------------------------------------- density compensation
  * Replaces ceilAndScale + countOccurrences + calculateR + calculateDcf
  * (vissgen3d_blockage.cu:105-141; the un-shifted formula of

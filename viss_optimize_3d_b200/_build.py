@@ -23,7 +23,7 @@ BUILD = os.path.join(PKG, "_build_obj")
 LIB = os.path.join(PKG, "libviss.so")
 BIN = os.path.join(PKG, "bin")
 
-CU_SOURCES = ["healpix.cu", "geometry.cu", "visibility.cu", "dcf.cu", "capi.cu"]
+CU_SOURCES = ["healpix.cu", "geometry.cu", "visibility.cu", "dcf.cu", "capi.cu", "noalloc.cu"]
 HEADERS = ["viss_common.cuh", "visibility.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -56,6 +56,15 @@ int fail(int status, const std::string &msg) {
   return status;
 }
 
+}  // namespace
+
+namespace viss {
+// Lets other translation units of the library record a failure message.
+int record_error(int status, const std::string &msg) { return fail(status, msg); }
+}  // namespace viss
+
+namespace {
+
 int cuda_fail(cudaError_t e, const char *where) {
   g_last_error = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
   return VISS_ERR_CUDA;

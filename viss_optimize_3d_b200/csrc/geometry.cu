@@ -275,4 +275,12 @@ cudaError_t sort_pixel_keys(long long J, unsigned long long *keys_in, unsigned l
   return e != cudaSuccess ? e : e2;
 }
 
+// Tile cones of already-staged pixel records (used by the allocation-free
+// forward entry point, which stages pixels in the caller's order).
+cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, double4 *cones, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  k_tile_cones<<<nblk(ntiles, 8), 256, 0, st>>>(ntiles, pix, cones);
+  return cudaGetLastError();
+}
+
 }  // namespace viss
