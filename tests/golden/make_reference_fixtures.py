@@ -1,0 +1,51 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures of tests/golden/ref_noblockage_10m/.
+
+Writes the small synthetic case of refcase.py in the reference's text formats,
+runs the reference's own vissgen3d_noblockage_10m program (built unmodified
+from its sources by oracle/build_ref.sh) on it -- on a GPU host, since the
+reference is CUDA-only -- and keeps its inputs, its output C1day1M.txt and
+its stdout (which prints Viss[0..2], the forward visibilities before the
+w-rotation).
+
+    python tests/golden/make_reference_fixtures.py --out DIR [--ref PATH]
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, ROOT)
+
+import refcase  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--ref", default=os.path.join(ROOT, "oracle", "_ref", "vissgen3d_noblockage_10m"))
+    args = ap.parse_args()
+    case = refcase.make_case()
+    with tempfile.TemporaryDirectory() as tmp:
+        refcase.write_inputs(case, tmp, variant_10m=True)
+        os.makedirs(os.path.join(tmp, "3dnoblockage10M"))
+        r = subprocess.run([args.ref], cwd=tmp, capture_output=True, text=True, timeout=600)
+        with open(os.path.join(tmp, "reference_stdout.txt"), "w") as f:
+            f.write(r.stdout)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
+            sys.exit(r.returncode)
+        out = os.path.abspath(args.out)
+        if os.path.exists(out):
+            shutil.rmtree(out)
+        shutil.copytree(tmp, out)
+    print("fixtures in", out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,79 @@
+"""The drop-in executables (same command lines, CWD-relative text inputs and
+output directories as the reference's vissgen3d_* and pix2ang programs) on a
+small synthetic case, against the FP64 oracle's restatement of vissGen
+(vissgen3d_blockage.cu:195-563).  Outputs are 6-significant-digit text, as the
+reference writes them (:549), so values are compared at 2e-5 of the largest."""
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "viss_optimize_3d_b200", "bin")
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+import refcase  # noqa: E402
+
+
+def run(exe, cwd, *args):
+    r = subprocess.run([os.path.join(BIN, exe), *args], cwd=cwd, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    return r.stdout
+
+
+def viss_lines(stdout):
+    out = []
+    for m in re.finditer(r"Viss\[(\d)\]: \(([^,]+),([^)]+)\)", stdout):
+        out.append(complex(float(m.group(2)), float(m.group(3))))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("exe,blockage", [("vissgen3d_noblockage_10m", False),
+                                          ("vissgen3d_blockage_10m", True)])
+def test_vissgen_10m(tmp_path, oracle, exe, blockage):
+    case = refcase.make_case()
+    refcase.write_inputs(case, str(tmp_path), variant_10m=True)
+    outdir = "3dblockage10M" if blockage else "3dnoblockage10M"
+    os.makedirs(tmp_path / outdir)
+    stdout = run(exe, tmp_path)                        # no arguments, like the reference
+    C = np.loadtxt(tmp_path / outdir / "C1day1M.txt")
+    V0, Co = refcase.oracle_vissgen(case, blockage)
+    assert C.shape == Co.shape
+    assert np.abs(C - Co).max() <= 2e-5 * np.abs(Co).max(), np.abs(C - Co).max()
+    V = viss_lines(stdout)
+    assert V.size == 3
+    np.testing.assert_allclose(V, V0[:3], rtol=2e-5, atol=2e-5 * np.abs(V0).max())
+    assert "npix: 192" in stdout and "total time:" in stdout
+
+
+def test_vissgen_1m_two_days(tmp_path, oracle):
+    case = refcase.make_case()
+    refcase.write_inputs(case, str(tmp_path), variant_10m=False)
+    os.makedirs(tmp_path / "3dblockage")
+    stdout = run("vissgen3d_blockage", tmp_path, "--days", "2")
+    C1 = np.loadtxt(tmp_path / "3dblockage" / "C1day1M.txt")
+    _, Co = refcase.oracle_vissgen(case, True, frequency=1e6)
+    assert np.abs(C1 - Co).max() <= 2e-5 * np.abs(Co).max()
+    # day 2 has no input files: zero rows, a zero image (as the reference)
+    C2 = np.loadtxt(tmp_path / "3dblockage" / "C2day1M.txt")
+    assert C2.shape == Co.shape and not C2.any()
+    assert "for loop: 2" in stdout
+
+
+def test_pix2ang_executable(tmp_path, oracle):
+    nside = 8
+    npix = 12 * nside * nside
+    with open(tmp_path / "B.txt", "w") as f:
+        f.write(f"{npix}\n" + "1.0\n" * npix)
+    run("pix2ang", tmp_path)
+    th = np.loadtxt(tmp_path / "theta_heal.txt")
+    ph = np.loadtxt(tmp_path / "phi_heal.txt")
+    oth, oph, _ = oracle.pix2ang(nside, nest=True)
+    np.testing.assert_allclose(th, oth.astype(np.float32), rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(ph, oph.astype(np.float32), rtol=1e-6, atol=1e-6)

@@ -117,53 +117,131 @@ __device__ long long ring2nest_one(long long N, long long p) {
   return -1;
 }
 
-// Angles and unit vector of one pixel centre.
+// ---------------------------------------------------------------- double-double
+// Unevaluated sums hi + lo (|lo| <= ulp(hi)/2) built from error-free
+// transformations (Dekker / Knuth two-sum, fma two-product).  Used only for
+// the pixel tables, to round every output correctly.
+struct dd {
+  double hi, lo;
+};
+
+__device__ __forceinline__ dd two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  const double bb = __dadd_rn(s, -a);
+  const double e = __dadd_rn(__dadd_rn(a, -__dadd_rn(s, -bb)), __dadd_rn(b, -bb));
+  return {s, e};
+}
+__device__ __forceinline__ dd quick_two_sum(double a, double b) {  // |a| >= |b|
+  const double s = __dadd_rn(a, b);
+  return {s, __dadd_rn(b, -__dadd_rn(s, a))};
+}
+__device__ __forceinline__ dd two_prod(double a, double b) {
+  const double p = __dmul_rn(a, b);
+  return {p, __fma_rn(a, b, -p)};
+}
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+  const dd s = two_sum(a.hi, b.hi);
+  return quick_two_sum(s.hi, __dadd_rn(s.lo, __dadd_rn(a.lo, b.lo)));
+}
+__device__ __forceinline__ dd dd_neg(dd a) { return {-a.hi, -a.lo}; }
+__device__ __forceinline__ dd dd_mul(dd a, dd b) {
+  dd p = two_prod(a.hi, b.hi);
+  p.lo = __dadd_rn(p.lo, __dadd_rn(__dmul_rn(a.hi, b.lo), __dmul_rn(a.lo, b.hi)));
+  return quick_two_sum(p.hi, p.lo);
+}
+__device__ __forceinline__ dd dd_div_d(dd a, double d) {
+  const double q1 = __ddiv_rn(a.hi, d);
+  const dd p = two_prod(q1, d);
+  const double r = __dadd_rn(__dadd_rn(__dadd_rn(a.hi, -p.hi), -p.lo), a.lo);
+  return quick_two_sum(q1, __ddiv_rn(r, d));
+}
+// exact integers a, b (|a|, |b| < 2^53) -> a / b
+__device__ __forceinline__ dd dd_ratio(double a, double b) { return dd_div_d({a, 0.0}, b); }
+__device__ __forceinline__ dd dd_sqrt(dd a) {
+  const double s = __dsqrt_rn(a.hi);
+  const dd p = two_prod(s, s);
+  const double r = __dadd_rn(__dadd_rn(__dadd_rn(a.hi, -p.hi), -p.lo), a.lo);
+  return quick_two_sum(s, __ddiv_rn(r, __dmul_rn(2.0, s)));
+}
+
+// pi and pi/2 as double-doubles
+__device__ __constant__ double c_pi_hi = 3.141592653589793116, c_pi_lo = 1.2246467991473532e-16;
+__device__ __constant__ double c_pio2_hi = 1.5707963267948966, c_pio2_lo = 6.123233995736766e-17;
+
+// sin and cos of a double-double x with |x| <= pi/4 + tiny, by their Taylor
+// series (the last term used is below 1e-33).
+__device__ void dd_sincos_small(dd x, dd &s, dd &c) {
+  const dd x2 = dd_mul(x, x);
+  dd ts = x, tc = {1.0, 0.0};
+  s = x;
+  c = {1.0, 0.0};
+  for (int n = 1; n <= 15; ++n) {
+    ts = dd_neg(dd_div_d(dd_mul(ts, x2), static_cast<double>((2 * n) * (2 * n + 1))));
+    tc = dd_neg(dd_div_d(dd_mul(tc, x2), static_cast<double>((2 * n - 1) * (2 * n))));
+    s = dd_add(s, ts);
+    c = dd_add(c, tc);
+  }
+}
+
+// (cos, sin) of k * pi/2 + a from (cos a, sin a): an exact quadrant rotation.
+__device__ __forceinline__ void quadrant(long long k, dd ca, dd sa, dd &c, dd &s) {
+  switch (static_cast<int>(((k % 4) + 4) % 4)) {
+    case 0: c = ca; s = sa; break;
+    case 1: c = dd_neg(sa); s = ca; break;
+    case 2: c = dd_neg(ca); s = dd_neg(sa); break;
+    default: c = sa; s = dd_neg(ca); break;
+  }
+}
+
+// Angles and unit vector of one pixel centre, every output correctly rounded
+// from double-double values: z and sin(theta) are exact rationals (rounded
+// once), phi = pi * nphi / den with pi as a double-double, cos/sin(phi) from
+// the exact quadrant of nphi/den, and theta = acos(z) corrected by one Newton
+// step on cos(theta) - z in double-double.
 __device__ void geo_angles(long long N, const PixGeo &g, double &theta, double &phi, double &x,
                            double &y, double &z) {
   const double dN = static_cast<double>(N);
-  double sth;
+  dd zd, s2;
   if (g.polar != 0) {
     const double nr = static_cast<double>(g.nr);
-    const double nr2 = nr * nr;           // exact (nr < 2^26)
-    const double d3 = 3.0 * dN * dN;      // exact
-    const double zabs = (d3 - nr2) / d3;  // one rounding
-    z = g.polar > 0 ? zabs : -zabs;
-    // sin^2 theta = nr^2 (6N^2 - nr^2) / (9 N^4); exact numerator / denominator
-    // while they stay below 2^53 (N <= 4096), else a two-step form.
-    const double six = 6.0 * dN * dN - nr2;
-    double s2;
-    if (N <= 4096) s2 = (nr2 * six) / (d3 * d3);
-    else s2 = (nr2 / d3) * (six / d3);
-    sth = sqrt(s2);
-    // angle from the pole: 2 asin(sqrt((1-|z|)/2)) = 2 asin(nr / (N sqrt 6))
-    const double half = 2.0 * asin(sqrt(nr2 / (2.0 * d3)));
-    if (g.polar > 0) {
-      theta = half;
-    } else {  // pi - half with pi as a double-double (fast two-sum, PI_HI > half)
-      const double t = 3.141592653589793116 - half;
-      const double e = (3.141592653589793116 - t) - half;
-      theta = t + (e + 1.2246467991473532e-16);
-    }
+    const double nr2 = nr * nr;       // exact (nr < 2^26)
+    const double d3 = 3.0 * dN * dN;  // exact
+    const dd omz = dd_ratio(nr2, d3);                       // 1 - |z|
+    const dd zabs = dd_add({1.0, 0.0}, dd_neg(omz));
+    zd = g.polar > 0 ? zabs : dd_neg(zabs);
+    s2 = dd_mul(omz, dd_ratio(6.0 * dN * dN - nr2, d3));    // sin^2 = omz (2 - omz)
   } else {
     const double d = 2.0 * dN - static_cast<double>(g.iring);  // exact
-    z = (2.0 * d) / (3.0 * dN);
-    const double nine = 9.0 * dN * dN;
-    sth = sqrt((nine - 4.0 * d * d) / nine);
-    theta = acos(z);
+    zd = dd_ratio(2.0 * d, 3.0 * dN);
+    s2 = dd_ratio(9.0 * dN * dN - 4.0 * d * d, 9.0 * dN * dN);
   }
-  // phi = nphi * pi / (4 nr) with pi = PI_HI + PI_LO (double-double)
-  const double nphi = static_cast<double>(2 * g.jp - g.kshift - 1);
-  const double den = static_cast<double>(4 * g.nr);
-  const double PI_HI = 3.141592653589793116, PI_LO = 1.2246467991473532e-16;
-  const double ph = nphi * PI_HI;
-  const double pl = fma(nphi, PI_HI, -ph) + nphi * PI_LO;  // nphi*pi = ph + pl
-  const double q1 = ph / den;
-  const double r = fma(-q1, den, ph) + pl;                  // exact remainder + low part
-  phi = q1 + r / den;
-  double sp, cp;
-  sincospi(nphi / den, &sp, &cp);
-  x = sth * cp;
-  y = sth * sp;
+  const dd sth = dd_sqrt(s2);
+  z = zd.hi;
+  // theta: acos, then one Newton step theta += (cos theta0 - z) / sin theta0
+  const double th0 = acos(zd.hi);
+  const long long kq = llrint(th0 / c_pio2_hi);
+  dd a = two_sum(th0, -static_cast<double>(kq) * c_pio2_hi);
+  a = dd_add(a, {-static_cast<double>(kq) * c_pio2_lo, 0.0});
+  dd ca, sa, ct, st;
+  dd_sincos_small(a, sa, ca);
+  quadrant(kq, ca, sa, ct, st);
+  const dd resid = dd_add(ct, dd_neg(zd));
+  theta = __dadd_rn(th0, __ddiv_rn(resid.hi, st.hi));
+  // phi = pi * nphi / den
+  const long long nphi = 2 * g.jp - g.kshift - 1, den = 4 * g.nr;
+  const dd pn = dd_add(two_prod(static_cast<double>(nphi), c_pi_hi),
+                       {__dmul_rn(static_cast<double>(nphi), c_pi_lo), 0.0});
+  phi = dd_div_d(pn, static_cast<double>(den)).hi;
+  // cos/sin(phi): phi = k pi/2 + r, r = pi (2 nphi - k den) / (2 den), |r| <= pi/4
+  const long long kp = (4 * nphi + den) / (2 * den);
+  const double m = static_cast<double>(2 * nphi - kp * den);
+  const dd r = dd_div_d(dd_add(two_prod(m, c_pi_hi), {__dmul_rn(m, c_pi_lo), 0.0}),
+                        2.0 * static_cast<double>(den));
+  dd cr, sr, cp, sp;
+  dd_sincos_small(r, sr, cr);
+  quadrant(kp, cr, sr, cp, sp);
+  x = dd_mul(sth, cp).hi;
+  y = dd_mul(sth, sp).hi;
 }
 
 __global__ void k_mk_pix2xy(int32_t *pix2x, int32_t *pix2y) {
