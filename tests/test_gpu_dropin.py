@@ -77,3 +77,19 @@ def test_pix2ang_executable(tmp_path, oracle):
     oth, oph, _ = oracle.pix2ang(nside, nest=True)
     np.testing.assert_allclose(th, oth.astype(np.float32), rtol=1e-6, atol=1e-6)
     np.testing.assert_allclose(ph, oph.astype(np.float32), rtol=1e-6, atol=1e-6)
+
+
+def test_noblockage_10m_reproduces_reference_output(tmp_path):
+    """Our drop-in on the inputs the reference program was run on
+    (tests/golden/ref_noblockage_10m) against the reference's own output."""
+    import shutil
+    fix = os.path.join(ROOT, "tests", "golden", "ref_noblockage_10m")
+    shutil.copytree(os.path.join(fix, "earth_10Mhz"), tmp_path / "earth_10Mhz")
+    os.makedirs(tmp_path / "3dnoblockage10M")
+    stdout = run("vissgen3d_noblockage_10m", tmp_path)
+    C = np.loadtxt(tmp_path / "3dnoblockage10M" / "C1day1M.txt")
+    Cref = np.loadtxt(os.path.join(fix, "3dnoblockage10M", "C1day1M.txt"))
+    assert np.abs(C - Cref).max() <= 2e-5 * np.abs(Cref).max()
+    ref_out = open(os.path.join(fix, "reference_stdout.txt")).read()
+    np.testing.assert_allclose(viss_lines(stdout), viss_lines(ref_out), rtol=2e-5,
+                               atol=2e-5 * np.abs(viss_lines(ref_out)).max())

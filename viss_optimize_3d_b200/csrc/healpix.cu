@@ -133,7 +133,7 @@ __device__ __forceinline__ dd two_sum(double a, double b) {
 }
 __device__ __forceinline__ dd quick_two_sum(double a, double b) {  // |a| >= |b|
   const double s = __dadd_rn(a, b);
-  return {s, __dadd_rn(b, -__dadd_rn(s, a))};
+  return {s, __dadd_rn(b, -__dadd_rn(s, -a))};
 }
 __device__ __forceinline__ dd two_prod(double a, double b) {
   const double p = __dmul_rn(a, b);
