@@ -245,6 +245,25 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return None
 
+    # the plain FP64 path on the same step (the split path's >= 3x target)
+    fp64 = None
+    if args.fp64_compare:
+        f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        f0.record(stream)
+        Vd = g.plan.forward(g.sky, fp64=True)
+        f1.record(stream)
+        g.plan.adjoint(coef, scale=2.0, mask=cfg.imaging_mask, fp64=True)
+        f2.record(stream)
+        torch.cuda.synchronize()
+        fp64_fwd, fp64_adj = f0.elapsed_time(f1) / 1e3, f1.elapsed_time(f2) / 1e3
+        split_fwd, split_adj = statistics.mean(fwd_ms) / 1e3, statistics.mean(adj_ms) / 1e3
+        Vs = g.plan.forward(g.sky).to(torch.complex128)
+        rel = (torch.linalg.norm(Vs - Vd.to(torch.complex128)) / torch.linalg.norm(Vd.to(torch.complex128))).item()
+        fp64 = {"value": round(terms_per_step / (fp64_fwd + fp64_adj) / 1e9, 3), "unit": UNIT,
+                "forward_ms": round(fp64_fwd * 1e3, 2), "adjoint_ms": round(fp64_adj * 1e3, 2),
+                "split_speedup": round((fp64_fwd + fp64_adj) / (split_fwd + split_adj), 2),
+                "forward_rel_l2_split_vs_fp64": float(f"{rel:.3e}")}
+
     pk, pk_kind = peaks()
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_terms = MUFU_TERMS_PER_CLK_PER_SM * nsm * pk["sm_max_mhz"] * 1e6
@@ -287,6 +306,7 @@ def run_ours(args, rank, world, local_rank):
         "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_mixed": round(mx_f / tot, 4),
                     "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_mixed": round(mx_a / tot, 4)},
         "gpu_launches": 10 * args.steps,
+        "fp64_path": fp64,
         "tuning": {"chosen": {"forward": shapes[0], "adjoint": shapes[1]},
                    "forward_shapes": "(samples/thread, CTAs/SM) = (4,2) (4,3) (2,3) (2,4)",
                    "adjoint_shapes": "(pixels/lane, CTAs/SM) = (8,2) (8,3) (4,3) (4,4)", **sweep},
@@ -379,6 +399,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false",
+                    help="skip timing the plain FP64 path on the same step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOAD_TEXT),
                     help="benchmark configuration (default: the headline one)")

@@ -75,8 +75,9 @@ def test_pix2ang_executable(tmp_path, oracle):
     th = np.loadtxt(tmp_path / "theta_heal.txt")
     ph = np.loadtxt(tmp_path / "phi_heal.txt")
     oth, oph, _ = oracle.pix2ang(nside, nest=True)
-    np.testing.assert_allclose(th, oth.astype(np.float32), rtol=1e-6, atol=1e-6)
-    np.testing.assert_allclose(ph, oph.astype(np.float32), rtol=1e-6, atol=1e-6)
+    # 6 significant digits of text: relative error up to 5e-6
+    np.testing.assert_allclose(th, oth.astype(np.float32), rtol=6e-6, atol=1e-6)
+    np.testing.assert_allclose(ph, oph.astype(np.float32), rtol=6e-6, atol=1e-6)
 
 
 def test_noblockage_10m_reproduces_reference_output(tmp_path):
