@@ -32,7 +32,12 @@
 //
 // Accuracy: terms are summed in FP32 within a tile / sample group (<= 128
 // terms per accumulator), those partial sums are folded into a
-// Kahan-compensated FP32 sum, and chunks are added in FP64.
+// Kahan-compensated FP32 sum, and chunks are added in FP64.  The SFU's sin and
+// cos carry a small mean error over a turn (~1e-8 on the B200); summed over
+// all pixels it would grow with the total flux rather than with |V|, which for
+// long baselines is ~700x smaller.  The split path therefore evaluates odd
+// pixel records half a turn further on and negates them (e^{i(x+pi)} = -e^{ix}),
+// so a constant SFU error cancels between neighbouring pixels.
 #include "visibility.cuh"
 
 namespace viss {
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   const int tid = threadIdx.x;
   const long long kb = static_cast<long long>(blockIdx.x) * (NT * R);
 
-  double ux[R], uy[R], uz[R], mk[R];
+  double ux[R], uy[R], uz[R], mk[R], mk2[R];
   bool kval[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -152,6 +157,7 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
     ux[r] = s.x; uy[r] = s.y; uz[r] = s.z;
     const double off = p.use_off ? s.w : 0.0;
     mk[r] = FP64 ? off : kMagic + off;
+    mk2[r] = FP64 ? off : kMagic + 0.5 + off;  // odd pixel records: half a turn on
     if (MASKED) s_refs[r][tid] = kval[r] ? p.refs[k] : make_int4(-1, -1, -1, -1);
   }
   unsigned nval_warp = 0;  // valid samples of this warp
@@ -227,14 +233,16 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
 #pragma unroll
       for (int r = 0; r < R; ++r) { t_re[r] = t_im[r] = 0.f; e_re[r] = e_im[r] = 0.0; }
       if (mode == 2) {
-#pragma unroll 2
-        for (int j = 0; j < kTilePix; ++j) {
-          const double4 q = tp[j];
-          const float I = sky_of(q);
+        for (int j = 0; j < kTilePix; j += 2) {
+          const double4 q0 = tp[j], q1 = tp[j + 1];
+          const float I0 = sky_of(q0);
+          const float I1 = FP64 ? sky_of(q1) : -sky_of(q1);
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
-            fwd_term<FP64>(t, I, t_re[r], t_im[r], e_re[r], e_im[r]);
+            const double t0 = fma(uz[r], q0.z, fma(uy[r], q0.y, fma(ux[r], q0.x, mk[r])));
+            fwd_term<FP64>(t0, I0, t_re[r], t_im[r], e_re[r], e_im[r]);
+            const double t1 = fma(uz[r], q1.z, fma(uy[r], q1.y, fma(ux[r], q1.x, mk2[r])));
+            fwd_term<FP64>(t1, I1, t_re[r], t_im[r], e_re[r], e_im[r]);
           }
         }
       } else {
@@ -245,16 +253,19 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
           if (st[r] == 2) {
             for (int j = 0; j < kTilePix; ++j) {
               const double4 q = tp[j];
-              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
-              fwd_term<FP64>(t, sky_of(q), t_re[r], t_im[r], e_re[r], e_im[r]);
+              const bool odd = !FP64 && (j & 1);
+              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, odd ? mk2[r] : mk[r])));
+              fwd_term<FP64>(t, odd ? -sky_of(q) : sky_of(q), t_re[r], t_im[r], e_re[r], e_im[r]);
             }
           } else {
             double4 q0, q1, q2;
             mixed_rows(s_refs[r][tid], st[r], p.occ, q0, q1, q2);
             for (int j = 0; j < kTilePix; ++j) {
               const double4 q = tp[j];
-              const float Iv = visible_rows(q0, q1, q2, q.x, q.y, q.z) ? sky_of(q) : 0.f;
-              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, mk[r])));
+              const bool odd = !FP64 && (j & 1);
+              float Iv = visible_rows(q0, q1, q2, q.x, q.y, q.z) ? sky_of(q) : 0.f;
+              if (odd) Iv = -Iv;
+              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, odd ? mk2[r] : mk[r])));
               fwd_term<FP64>(t, Iv, t_re[r], t_im[r], e_re[r], e_im[r]);
             }
           }
@@ -421,6 +432,10 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
 
   unsigned long long evaluated = 0, mixed_terms = 0;
   const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
+  // odd pixel records (odd lanes: record index = pbase + 32 q + lane) are
+  // evaluated half a turn on and negated at the end (see the file comment)
+  const bool odd_lane = (lane & 1) != 0;
+  const double magic = odd_lane ? kMagic + 0.5 : kMagic;
   for (int it = 0; it < ntile; ++it) {
     const int buf = it & 1;
     const uint32_t par = (it >> 1) & 1;
@@ -460,7 +475,7 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
         const double4 u = sp[g + i];
         const float2 a = cp[g + i];
         const double uoff = p.use_off ? u.w : 0.0;
-        adj_sample<P, false, FP64>(u, FP64 ? uoff : kMagic + uoff, a, sx, sy, sz, pass, pass,
+        adj_sample<P, false, FP64>(u, FP64 ? uoff : magic + uoff, a, sx, sy, sz, pass, pass,
                                    pass, t_acc, e_acc);
       }
       // samples that need the per-pixel occultation test
@@ -472,7 +487,7 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
         const double uoff = p.use_off ? u.w : 0.0;
         double4 q0, q1, q2;
         mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
-        adj_sample<P, true, FP64>(u, FP64 ? uoff : kMagic + uoff, a, sx, sy, sz, q0, q1, q2,
+        adj_sample<P, true, FP64>(u, FP64 ? uoff : magic + uoff, a, sx, sy, sz, q0, q1, q2,
                                   t_acc, e_acc);
       }
     }
@@ -503,8 +518,10 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     const long long j = pbase + q * 32 + lane;
-    out[j] = FP64 ? dacc[q]
-                  : static_cast<double>(s_kahan[0][q][tid]) - static_cast<double>(s_kahan[1][q][tid]);
+    const double sum =
+        FP64 ? dacc[q]
+             : static_cast<double>(s_kahan[0][q][tid]) - static_cast<double>(s_kahan[1][q][tid]);
+    out[j] = (!FP64 && odd_lane) ? -sum : sum;
   }
 }
 
