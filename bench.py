@@ -114,7 +114,7 @@ class ClockSampler:
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
-    from viss_optimize_3d_b200 import pipeline, synth, api
+    from viss_optimize_3d_b200 import api, pipeline, replicas, synth
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -124,7 +124,9 @@ def run_ours(args, rank, world, local_rank):
         cfg = synth.CONFIGS[args.workload]
     if world > 1:
         import dataclasses
-        cfg = dataclasses.replace(cfg, day=float(rank))     # one observation day per replica
+        # one observation day per replica, the reference's round-robin day split
+        day = replicas.days_for_rank(world, rank, world)[0]
+        cfg = dataclasses.replace(cfg, day=float(day - 1))
     f_hz = cfg.freqs_hz[0]
     obs = synth.make_observation(cfg)
     g = pipeline.upload(obs, f_hz, device=dev)
@@ -237,11 +239,8 @@ def run_ours(args, rank, world, local_rank):
     h2d = J * 4 + K * 24 + K * 12
     d2h = J * 4 + K * 8
 
-    # max over ranks
-    t = torch.tensor([total_s, e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_s, e2e_s = t.tolist()
+    # max over ranks (device-timed seconds)
+    total_s, e2e_s = replicas.max_over_ranks([total_s, e2e_s], device=dev)
     if rank != 0:
         return None
 
