@@ -143,6 +143,15 @@ int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, 
  * cudaOccupancyMaxPotentialBlockSize, vissgen3d_blockage.cu:412-413). */
 int viss_plan_tune(viss_plan *plan, const float *sky, const float *coef, float *V_scratch,
                    float *img_scratch, int flags, int *fwd_shape, int *adj_shape, void *stream);
+/* Frequency channels: the plan's K samples are `channels` consecutive blocks
+ * of K/channels samples (the same baselines at each frequency; K/channels even
+ * when channels > 1).  viss_forward then takes sky as channels x J (one map
+ * per channel) and viss_adjoint writes image as channels x J; V and coef stay
+ * K long.  All channels run in one launch of each kernel.  viss_plan_set_samples
+ * resets the plan to one channel.  No counterpart in the reference (it runs one
+ * frequency per executable, vissgen3d_blockage.cu:568). */
+int viss_plan_set_channels(viss_plan *plan, int channels);
+
 /* Sets the launch shapes directly (indices 0..3 each). */
 int viss_plan_set_shapes(viss_plan *plan, int fwd_shape, int adj_shape);
 

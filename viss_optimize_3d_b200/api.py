@@ -140,7 +140,7 @@ class Plan:
     occ  (G, 4) FP64 occulter table
     """
 
-    def __init__(self, lmn, uvw, off=None, refs=None, occ=None):
+    def __init__(self, lmn, uvw, off=None, refs=None, occ=None, channels: int = 1):
         self._h = C.c_void_p()
         check(lib.viss_plan_create(C.byref(self._h)), "viss_plan_create")
         lmn = _cuda(lmn, torch.float64, shape_last=3)
@@ -156,6 +156,15 @@ class Plan:
                                         0 if occ is None else occ.shape[0], _p(occ), st),
               "viss_plan_set_samples")
         self.masked = refs is not None
+        self.channels = 1
+        if channels != 1:
+            self.set_channels(channels)
+
+    def set_channels(self, channels: int):
+        """Split the samples into `channels` consecutive equal blocks, one per
+        frequency; sky and image become (channels, J)."""
+        check(lib.viss_plan_set_channels(self._h, int(channels)), "viss_plan_set_channels")
+        self.channels = int(channels)
 
     @staticmethod
     def _flags(fp64, mask, use_offset, accumulate=False):
@@ -175,8 +184,8 @@ class Plan:
         """healpix_moonback_viss (vissgen3d_blockage.cu:76-102):
         V_k = sum_j sky_j vis_kj exp(-2 pi i (u_k.s_j + off_k)), complex64."""
         sky = _cuda(sky, torch.float32, self.device)
-        if sky.shape != (self.J,):
-            raise ValueError(f"sky must have shape ({self.J},)")
+        if sky.numel() != self.channels * self.J:
+            raise ValueError(f"sky must hold {self.channels} x {self.J} values")
         if out is None:
             out = torch.empty(self.K, dtype=torch.complex64, device=self.device)
         check(lib.viss_forward(self._h, _p(sky), _p(out), self._flags(fp64, mask, use_offset),
@@ -191,7 +200,8 @@ class Plan:
         if coef.shape != (self.K,):
             raise ValueError(f"coef must have shape ({self.K},)")
         if out is None:
-            out = torch.empty(self.J, dtype=torch.float32, device=self.device)
+            shape = (self.J,) if self.channels == 1 else (self.channels, self.J)
+            out = torch.empty(shape, dtype=torch.float32, device=self.device)
         check(lib.viss_adjoint(self._h, _p(coef), _p(out), float(scale),
                                self._flags(fp64, mask, use_offset), _stream(coef)), "viss_adjoint")
         return out

@@ -32,7 +32,7 @@ cudaError_t sort_pixel_keys(long long, unsigned long long *, unsigned long long 
 cudaError_t launch_stage_pixels(long long, long long, const double *, const int *, double4 *,
                                 double4 *, cudaStream_t);
 cudaError_t launch_stage_sky(long long, long long, const double4 *, const int *, const float *,
-                             float, double4 *, cudaStream_t);
+                             float, double4 *, int, cudaStream_t);
 cudaError_t launch_stage_coef(long long, long long, const float2 *, float2 *, cudaStream_t);
 cudaError_t launch_stage_samples(long long, const double *, const double *, const int32_t *,
                                  double4 *, int4 *, unsigned long long *, cudaStream_t);
@@ -115,6 +115,8 @@ struct viss_plan {
   int *perm = nullptr;       size_t perm_cap = 0;  // record i holds caller pixel perm[i]
   // samples
   long long K = 0, Kpad = 0;
+  int channels = 1;        // channel-major sample axis: K = channels * Kc
+  long long Kc = 0;
   double4 *samp = nullptr; size_t samp_cap = 0;
   int4 *refs = nullptr;    size_t refs_cap = 0;
   bool has_refs = false;
@@ -141,23 +143,26 @@ namespace {
 
 int fwd_chunks(const viss_plan *p, int shape, bool fp64) {
   const long long per = viss::forward_samples_per_block(shape, fp64);
-  const long long blocks = (p->K + per - 1) / per;
+  const long long blocks = (p->Kc + per - 1) / per * p->channels;
   const long long slots = static_cast<long long>(p->nsm) * viss::forward_ctas_per_sm(shape, fp64);
   long long c = (static_cast<long long>(p->fwd_waves) * slots + blocks - 1) / blocks;
   c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 2)));
   return static_cast<int>(c);
 }
 
+// Sample chunks per channel for the adjoint (and their size, a multiple of
+// the staging tile).
 int adj_chunks(const viss_plan *p, int shape, bool fp64, int *samples_per_chunk) {
   const long long per = viss::adjoint_pixels_per_block(shape, fp64);  // pixels per CTA
-  const long long blocks = (p->Jpad + per - 1) / per;
+  const long long blocks = (p->Jpad + per - 1) / per * p->channels;
   const long long slots = static_cast<long long>(p->nsm) * viss::adjoint_ctas_per_sm(shape, fp64);
   long long c = (static_cast<long long>(p->adj_waves) * slots + blocks - 1) / blocks;
-  const long long max_c = std::max<long long>(1, (p->K + 255) / 256);
+  const long long max_c = std::max<long long>(1, (p->Kc + 255) / 256);
   c = std::max<long long>(1, std::min(c, max_c));
-  long long spc = (p->K + c - 1) / c;
+  c = std::min<long long>(c, std::max<long long>(1, 65535 / p->channels));
+  long long spc = (p->Kc + c - 1) / c;
   spc = (spc + viss::kSampTile - 1) / viss::kSampTile * viss::kSampTile;
-  c = (p->K + spc - 1) / spc;
+  c = (p->Kc + spc - 1) / spc;
   *samples_per_chunk = static_cast<int>(spc);
   return static_cast<int>(std::max<long long>(1, c));
 }
@@ -370,6 +375,8 @@ int viss_plan_set_samples(viss_plan *p, int64_t K, const double *uvw, const doub
     return fail(VISS_ERR_NOTFINITE, "viss_plan_set_samples: non-finite uvw or offset");
   p->K = K;
   p->Kpad = Kpad;
+  p->channels = 1;
+  p->Kc = K;
   p->has_refs = refs != nullptr;
   p->G = refs ? G : 0;
   p->max_turns = bound;
@@ -386,7 +393,11 @@ static int forward_impl(viss_plan *p, const float *sky, float *V, int flags, cud
   const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
   const int nchunk = fwd_chunks(p, shape, fp64);
   if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * p->K)) return s;
-  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, st),
+  if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * p->Jpad * p->channels,
+                     "pixel+sky records"))
+    return s;
+  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky,
+                                   p->channels, st),
             "viss_forward: sky");
   VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_forward");
   viss::FwdParams fp;
@@ -403,6 +414,9 @@ static int forward_impl(viss_plan *p, const float *sky, float *V, int flags, cud
   fp.counter = p->dev_words;
   fp.err = reinterpret_cast<int *>(p->dev_words + 1);
   fp.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
+  fp.channels = p->channels;
+  fp.Kc = p->Kc;
+  fp.pix_stride = p->Jpad;
   VISS_CUDA(viss::launch_forward(fp, shape, real_chunks, masked, fp64, st), "viss_forward: kernel");
   VISS_CUDA(viss::launch_reduce_fwd(p->K, real_chunks, fp.part, reinterpret_cast<float2 *>(V),
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
@@ -432,7 +446,8 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
   const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
   int spc = 0;
   const int nchunk = adj_chunks(p, shape, fp64, &spc);
-  if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->Jpad)) return s;
+  if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->channels * p->Jpad))
+    return s;
   VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
             "viss_adjoint: coef");
   VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_adjoint");
@@ -450,8 +465,11 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
   ap.counter = p->dev_words;
   ap.err = reinterpret_cast<int *>(p->dev_words + 1);
   ap.use_off = (flags & VISS_NO_OFFSET) ? 0 : 1;
+  ap.channels = p->channels;
+  ap.Kc = p->Kc;
+  ap.nchunk = nchunk;
   VISS_CUDA(viss::launch_adjoint(ap, shape, nchunk, masked, fp64, st), "viss_adjoint: kernel");
-  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, ap.part, p->perm, scale, image,
+  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, p->channels, ap.part, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_adjoint: reduce");
   p->last_total = p->K * p->J;
@@ -507,6 +525,20 @@ int viss_plan_tune(viss_plan *p, const float *sky, const float *coef, float *V_s
   p->adj_shape = ba;
   if (fwd_shape) *fwd_shape = bf;
   if (adj_shape) *adj_shape = ba;
+  return VISS_OK;
+}
+
+int viss_plan_set_channels(viss_plan *p, int channels) {
+  if (!p || channels < 1) return fail(VISS_ERR_ARG, "viss_plan_set_channels: bad arguments");
+  if (p->K <= 0) return fail(VISS_ERR_STATE, "viss_plan_set_channels: samples not set");
+  if (p->K % channels != 0)
+    return fail(VISS_ERR_ARG, "viss_plan_set_channels: the sample count is not a multiple of channels");
+  const long long Kc = p->K / channels;
+  if (channels > 1 && (Kc & 1))
+    return fail(VISS_ERR_ARG, "viss_plan_set_channels: samples per channel must be even");
+  if (channels > 65535) return fail(VISS_ERR_ARG, "viss_plan_set_channels: at most 65535 channels");
+  p->channels = channels;
+  p->Kc = Kc;
   return VISS_OK;
 }
 

@@ -153,14 +153,16 @@ __global__ void k_tile_cones(long long ntiles, const double4 *pix, double4 *cone
 
 // Sky staging: pixel record + sky value in the low word of .w (zero past J),
 // so one 32-byte record per pixel carries everything the forward reads.
+// One channel per blockIdx.y: out[ch][i] = (pix[i], sky[ch][perm[i]]).
 __global__ void k_stage_sky(long long J, long long Jpad, const double4 *pix, const int *perm,
                             const float *sky, float scale, double4 *out) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= Jpad) return;
+  const long long ch = blockIdx.y;
   double4 r = pix[i];
-  const float v = i < J ? __fmul_rn(sky[perm[i]], scale) : 0.0f;
+  const float v = i < J ? __fmul_rn(sky[ch * J + perm[i]], scale) : 0.0f;
   r.w = __hiloint2double(0, __float_as_int(v));
-  out[i] = r;
+  out[ch * Jpad + i] = r;
 }
 
 // Sample staging: uvw (K x 3), off (K or null), refs (K x 3 or null).
@@ -228,8 +230,10 @@ cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, 
 }
 
 cudaError_t launch_stage_sky(long long J, long long Jpad, const double4 *pix, const int *perm,
-                             const float *sky, float scale, double4 *out, cudaStream_t st) {
-  k_stage_sky<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, pix, perm, sky, scale, out);
+                             const float *sky, float scale, double4 *out, int channels,
+                             cudaStream_t st) {
+  dim3 grid(nblk(Jpad, 256), static_cast<unsigned>(channels));
+  k_stage_sky<<<grid, 256, 0, st>>>(J, Jpad, pix, perm, sky, scale, out);
   return cudaGetLastError();
 }
 

@@ -192,6 +192,9 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   fp.counter = words;
   fp.err = reinterpret_cast<int *>(words + 1);
   fp.use_off = 1;
+  fp.channels = 1;
+  fp.Kc = K;
+  fp.pix_stride = Jpad;
   if ((e = viss::launch_forward(fp, shape, real_chunks, refs != nullptr, false, st)) != cudaSuccess)
     return na_cuda(e, "forward kernel");
   if ((e = viss::launch_reduce_fwd(K, real_chunks, part, reinterpret_cast<float2 *>(V), 0, st)) !=

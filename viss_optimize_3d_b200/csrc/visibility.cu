@@ -145,14 +145,19 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
-  const long long kb = static_cast<long long>(blockIdx.x) * (NT * R);
+  // CTAs never straddle channels: blockIdx.x = channel * blocks_per_channel + block
+  const long long bpc = (p.Kc + NT * R - 1) / (NT * R);
+  const long long ch = blockIdx.x / bpc;
+  const long long kloc = (blockIdx.x - ch * bpc) * (NT * R);   // first sample in the channel
+  const long long kb = ch * p.Kc + kloc;
+  const double4 *pix = p.pix + ch * p.pix_stride;               // this channel's sky records
 
   double ux[R], uy[R], uz[R], mk[R], mk2[R];
   bool kval[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const long long k = kb + r * NT + tid;
-    kval[r] = k < p.K;
+    kval[r] = kloc + r * NT + tid < p.Kc;
     const double4 s = kval[r] ? p.samp[k] : make_double4(0, 0, 0, 0);
     ux[r] = s.x; uy[r] = s.y; uz[r] = s.z;
     const double off = p.use_off ? s.w : 0.0;
@@ -185,7 +190,7 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   __syncthreads();
   if (tid == 0 && t0 < t1) {
     mbar_expect_tx(&s_bar[0], kTileBytes);
-    bulk_g2s(s_pix[0], p.pix + static_cast<long long>(t0) * kTilePix, kTileBytes, &s_bar[0]);
+    bulk_g2s(s_pix[0], pix + static_cast<long long>(t0) * kTilePix, kTileBytes, &s_bar[0]);
   }
 
   unsigned long long evaluated = 0, mixed_terms = 0;
@@ -195,7 +200,7 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
     const uint32_t par = (it >> 1) & 1;
     if (tid == 0 && t + 1 < t1) {
       mbar_expect_tx(&s_bar[buf ^ 1], kTileBytes);
-      bulk_g2s(s_pix[buf ^ 1], p.pix + static_cast<long long>(t + 1) * kTilePix, kTileBytes,
+      bulk_g2s(s_pix[buf ^ 1], pix + static_cast<long long>(t + 1) * kTilePix, kTileBytes,
                &s_bar[buf ^ 1]);
     }
     // classify the tile for this warp's samples
@@ -405,8 +410,10 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
     if (!FP64) s_kahan[0][q][tid] = s_kahan[1][q][tid] = 0.f;
   }
 
-  const long long k0 = static_cast<long long>(blockIdx.y) * p.samples_per_chunk;
-  const long long k1 = min(k0 + p.samples_per_chunk, p.K);
+  // blockIdx.y = channel * nchunk + chunk; a chunk never leaves its channel
+  const long long ch = blockIdx.y / p.nchunk;
+  const long long k0 = ch * p.Kc + static_cast<long long>(blockIdx.y - ch * p.nchunk) * p.samples_per_chunk;
+  const long long k1 = min(k0 + p.samples_per_chunk, (ch + 1) * p.Kc);
   const int ntile = static_cast<int>((k1 - k0 + kSampTile - 1) / kSampTile);
 
   auto issue = [&](int it, int buf) {
@@ -525,11 +532,14 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   }
 }
 
-// image[perm[i]] = scale * sum over chunks of record i (FP64).
+// image[ch][perm[i]] = scale * sum over the channel's chunks of record i (FP64).
 __global__ void k_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
                              const int *perm, float scale, float *img, int accumulate) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= J) return;
+  const long long ch = blockIdx.y;
+  part += ch * nchunk * Jpad;
+  img += ch * J;
   double s = 0;
   for (int c = 0; c < nchunk; ++c) s += part[static_cast<long long>(c) * Jpad + i];
   s *= static_cast<double>(scale);
@@ -554,8 +564,9 @@ const AdjShape kAdjShapes[kNumAdjShapes] = {{8, 2}, {8, 3}, {4, 3}, {4, 4}};
 template <int R, int MINB, bool M, bool F>
 static cudaError_t fwd_inst(const FwdParams &p, int nchunk, cudaStream_t st) {
   const long long per = static_cast<long long>(kFwdNT) * R;
-  const unsigned gx = static_cast<unsigned>((p.K + per - 1) / per);
-  dim3 grid(gx, nchunk);
+  const long long gx = (p.Kc + per - 1) / per * p.channels;
+  if (gx > 0x7fffffffLL) return cudaErrorInvalidValue;
+  dim3 grid(static_cast<unsigned>(gx), nchunk);
   k_forward<kFwdNT, R, MINB, M, F><<<grid, kFwdNT, 0, st>>>(p);
   return cudaGetLastError();
 }
@@ -607,7 +618,9 @@ template <int P, int MINB, bool M, bool F>
 static cudaError_t adj_inst(const AdjParams &p, int nchunk, cudaStream_t st) {
   const long long pix_per_cta = static_cast<long long>(kAdjNT / 32) * 32 * P;
   const unsigned gx = static_cast<unsigned>((p.Jpad + pix_per_cta - 1) / pix_per_cta);
-  dim3 grid(gx, nchunk);
+  const long long gy = static_cast<long long>(nchunk) * p.channels;
+  if (gy > 65535) return cudaErrorInvalidValue;
+  dim3 grid(gx, static_cast<unsigned>(gy));
   k_adjoint<kAdjNT, P, MINB, M, F><<<grid, kAdjNT, 0, st>>>(p);
   return cudaGetLastError();
 }
@@ -630,11 +643,12 @@ cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool maske
   }
 }
 
-cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
-                              const int *perm, float scale, float *img, int acc, cudaStream_t st) {
+cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, int channels,
+                              const double *part, const int *perm, float scale, float *img, int acc,
+                              cudaStream_t st) {
   if (J <= 0) return cudaSuccess;
-  k_reduce_adj<<<static_cast<unsigned>((J + 255) / 256), 256, 0, st>>>(J, Jpad, nchunk, part,
-                                                                        perm, scale, img, acc);
+  dim3 grid(static_cast<unsigned>((J + 255) / 256), static_cast<unsigned>(channels));
+  k_reduce_adj<<<grid, 256, 0, st>>>(J, Jpad, nchunk, part, perm, scale, img, acc);
   return cudaGetLastError();
 }
 

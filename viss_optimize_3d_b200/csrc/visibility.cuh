@@ -21,6 +21,9 @@ struct FwdParams {
   unsigned long long *counter;  // [0] exponentials evaluated, [2] of them in mixed tiles
   int *err;
   int use_off;                  // add the per-sample offset (.w) to the phase
+  int channels;                 // channel-major sample axis: K = channels * Kc
+  long long Kc;                 // samples per channel
+  long long pix_stride;         // pixel records per channel's sky (Jpad)
 };
 
 struct AdjParams {
@@ -37,6 +40,9 @@ struct AdjParams {
   unsigned long long *counter;
   int *err;
   int use_off;                  // add the per-sample offset (.w) to the phase
+  int channels;                 // one image per channel; K = channels * Kc
+  long long Kc;                 // samples per channel (even when channels > 1)
+  int nchunk;                   // sample chunks per channel (gridDim.y = channels * nchunk)
 };
 
 struct FwdShape { int R, minb; };
@@ -56,7 +62,8 @@ cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool maske
                            cudaStream_t st);
 int adjoint_pixels_per_block(int shape, bool fp64);
 int adjoint_ctas_per_sm(int shape, bool fp64);
-cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, const double *part,
-                              const int *perm, float scale, float *img, int acc, cudaStream_t st);
+cudaError_t launch_reduce_adj(long long J, long long Jpad, int nchunk, int channels,
+                              const double *part, const int *perm, float scale, float *img, int acc,
+                              cudaStream_t st);
 
 }  // namespace viss
