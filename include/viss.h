@@ -135,9 +135,9 @@ int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, 
 
 /* Autotuner: times every launch shape of the forward and adjoint kernels on
  * this plan's problem (CUDA events on `stream`, one warm-up and one timed
- * launch each) and keeps the fastest for later calls.  sky (J FP32) and coef
- * (K complex64) are representative inputs; V_scratch (K complex64) and
- * img_scratch (J FP32) receive throw-away outputs.  Synchronous.  The chosen
+ * launch each) and keeps the fastest for later calls.  sky (channels x J
+ * FP32) and coef (K complex64) are representative inputs; V_scratch (K
+ * complex64) and img_scratch (channels x J FP32) receive throw-away outputs.  Synchronous.  The chosen
  * shape indices are returned through fwd_shape / adj_shape (may be NULL).
  * No counterpart in the reference (it launches one fixed shape from
  * cudaOccupancyMaxPotentialBlockSize, vissgen3d_blockage.cu:412-413). */

@@ -219,8 +219,10 @@ class Plan:
         if coef is None:
             coef = torch.ones(self.K, dtype=torch.complex64, device=self.device)
         coef = _cuda(coef, torch.complex64, self.device)
+        if sky.numel() != self.channels * self.J or coef.numel() != self.K:
+            raise ValueError("tune: sky must hold channels x J values and coef K values")
         V = torch.empty(self.K, dtype=torch.complex64, device=self.device)
-        img = torch.empty(self.J, dtype=torch.float32, device=self.device)
+        img = torch.empty(self.channels * self.J, dtype=torch.float32, device=self.device)
         fs, as_ = C.c_int(), C.c_int()
         check(lib.viss_plan_tune(self._h, _p(sky), _p(coef), _p(V), _p(img),
                                  self._flags(False, mask, use_offset), C.byref(fs), C.byref(as_),
