@@ -188,6 +188,9 @@ class Plan:
             raise ValueError(f"sky must hold {self.channels} x {self.J} values")
         if out is None:
             out = torch.empty(self.K, dtype=torch.complex64, device=self.device)
+        elif (out.dtype != torch.complex64 or not out.is_contiguous() or out.numel() != self.K
+              or out.device != self.device):
+            raise ValueError(f"out must be a contiguous complex64 tensor of {self.K} values on {self.device}")
         check(lib.viss_forward(self._h, _p(sky), _p(out), self._flags(fp64, mask, use_offset),
                                _stream(sky)), "viss_forward")
         return out
@@ -202,6 +205,10 @@ class Plan:
         if out is None:
             shape = (self.J,) if self.channels == 1 else (self.channels, self.J)
             out = torch.empty(shape, dtype=torch.float32, device=self.device)
+        elif (out.dtype != torch.float32 or not out.is_contiguous()
+              or out.numel() != self.channels * self.J or out.device != self.device):
+            raise ValueError(f"out must be a contiguous float32 tensor of {self.channels} x {self.J} "
+                             f"values on {self.device}")
         check(lib.viss_adjoint(self._h, _p(coef), _p(out), float(scale),
                                self._flags(fp64, mask, use_offset), _stream(coef)), "viss_adjoint")
         return out
