@@ -140,25 +140,35 @@ class Plan:
     occ  (G, 4) FP64 occulter table
     """
 
-    def __init__(self, lmn, uvw, off=None, refs=None, occ=None, channels: int = 1):
+    def __init__(self, lmn, uvw=None, off=None, refs=None, occ=None, channels: int = 1):
         self._h = C.c_void_p()
         check(lib.viss_plan_create(C.byref(self._h)), "viss_plan_create")
         lmn = _cuda(lmn, torch.float64, shape_last=3)
         self.device = lmn.device
+        self.J = lmn.shape[0]
+        self.K = 0
+        self.channels = 1
+        self.masked = False
+        check(lib.viss_plan_set_pixels(self._h, self.J, _p(lmn), _stream(lmn)), "viss_plan_set_pixels")
+        if uvw is not None:
+            self.set_samples(uvw, off, refs, occ)
+        if channels != 1:
+            self.set_channels(channels)
+
+    def set_samples(self, uvw, off=None, refs=None, occ=None):
+        """(Re)stage the samples; resets the plan to one channel.  Synchronises
+        the stream once (it checks the phase bound of the split path)."""
         uvw = _cuda(uvw, torch.float64, self.device, shape_last=3)
         off = _cuda(off, torch.float64, self.device)
         refs = _cuda(refs, torch.int32, self.device, shape_last=3)
         occ = _cuda(occ, torch.float64, self.device, shape_last=4) if refs is not None else None
-        self.J, self.K = lmn.shape[0], uvw.shape[0]
-        st = _stream(lmn)
-        check(lib.viss_plan_set_pixels(self._h, self.J, _p(lmn), st), "viss_plan_set_pixels")
-        check(lib.viss_plan_set_samples(self._h, self.K, _p(uvw), _p(off), _p(refs),
-                                        0 if occ is None else occ.shape[0], _p(occ), st),
+        K = uvw.shape[0]
+        check(lib.viss_plan_set_samples(self._h, K, _p(uvw), _p(off), _p(refs),
+                                        0 if occ is None else occ.shape[0], _p(occ), _stream(uvw)),
               "viss_plan_set_samples")
+        self.K = K
         self.masked = refs is not None
         self.channels = 1
-        if channels != 1:
-            self.set_channels(channels)
 
     def set_channels(self, channels: int):
         """Split the samples into `channels` consecutive equal blocks, one per
