@@ -170,9 +170,10 @@ int viss_plan_last_stats(viss_plan *plan, int64_t *evaluated, int64_t *mixed, in
  * allocate after start-up).  No counterpart in the reference.  Same result
  * as viss_forward (split precision) for lmn (J x 3), sky (J), uvw (K x 3),
  * off (K or NULL), refs (K x 3 or NULL) and occ (G x 4, 16-byte aligned);
- * V is K complex64.  All intermediates live in one fixed 7.5 MiB __device__
+ * V is K complex64.  All intermediates live in one fixed 9 MiB __device__
  * array that every GPU loading the library holds until the process exits.
- * Limits: J <= 65536 pixels, K <= 32768 samples (else VISS_ERR_ARG).  The
+ * Limits: J <= 65536 pixels, K <= 32768 samples, G <= 98304 occulter rows
+ * (else VISS_ERR_ARG).  The
  * first call on a device looks up the array's address (cudaGetSymbolAddress)
  * -- make it before any stream capture.  Calls share the array: calls that
  * overlap on the GPU race.  Each call synchronises `stream` once. */

@@ -30,7 +30,8 @@ cudaError_t launch_pix_keys(long long, const double *, unsigned long long *, int
 cudaError_t sort_pixel_keys(long long, unsigned long long *, unsigned long long *, int *, int *,
                             cudaStream_t);
 cudaError_t launch_stage_pixels(long long, long long, const double *, const int *, double4 *,
-                                double4 *, cudaStream_t);
+                                float4 *, cudaStream_t);
+cudaError_t launch_occ32(long long, const double4 *, float4 *, cudaStream_t);
 cudaError_t launch_stage_sky(long long, long long, const double4 *, const int *, const float *,
                              float, double4 *, int, cudaStream_t);
 cudaError_t launch_stage_coef(long long, long long, const float2 *, float2 *, cudaStream_t);
@@ -111,7 +112,7 @@ struct viss_plan {
   int ntiles = 0;
   double4 *pix = nullptr;    size_t pix_cap = 0;
   double4 *pixsky = nullptr; size_t pixsky_cap = 0;
-  double4 *cones = nullptr;  size_t cones_cap = 0;
+  float4 *cones = nullptr;   size_t cones_cap = 0;  // tile cones, then sub-tile cones
   int *perm = nullptr;       size_t perm_cap = 0;  // record i holds caller pixel perm[i]
   // samples
   long long K = 0, Kpad = 0;
@@ -121,6 +122,7 @@ struct viss_plan {
   int4 *refs = nullptr;    size_t refs_cap = 0;
   bool has_refs = false;
   double4 *occ = nullptr;  size_t occ_cap = 0;
+  float4 *occ32 = nullptr; size_t occ32_cap = 0;  // classification rows
   long long G = 0;
   float2 *coef = nullptr;  size_t coef_cap = 0;
   double max_turns = 0;
@@ -305,8 +307,8 @@ int viss_plan_create(viss_plan **plan) {
 
 int viss_plan_destroy(viss_plan *p) {
   if (!p) return VISS_OK;
-  void *bufs[] = {p->pix, p->pixsky, p->cones, p->perm, p->samp, p->refs, p->occ, p->coef, p->part,
-                  p->dev_words};
+  void *bufs[] = {p->pix,  p->pixsky, p->cones, p->perm, p->samp,     p->refs,
+                  p->occ,  p->occ32,  p->coef,  p->part, p->dev_words};
   for (void *b : bufs)
     if (b) cudaFree(b);
   delete p;
@@ -322,7 +324,7 @@ int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *strea
   const long long nt = Jpad / viss::kTilePix;
   if (int s = ensure(p->pix, p->pix_cap, sizeof(double4) * Jpad, "pixel records")) return s;
   if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * Jpad, "pixel+sky records")) return s;
-  if (int s = ensure(p->cones, p->cones_cap, sizeof(double4) * nt, "tile cones")) return s;
+  if (int s = ensure(p->cones, p->cones_cap, sizeof(float4) * 5 * nt, "tile cones")) return s;
   if (int s = ensure(p->perm, p->perm_cap, sizeof(int) * J, "pixel order")) return s;
   const cudaStream_t st = as_stream(stream);
   // compact tiles: order the pixels by a hierarchical (NESTED) locality key
@@ -357,8 +359,10 @@ int viss_plan_set_samples(viss_plan *p, int64_t K, const double *uvw, const doub
   if (refs) {
     if (int s = ensure(p->refs, p->refs_cap, sizeof(int4) * Kpad, "occulter refs")) return s;
     if (int s = ensure(p->occ, p->occ_cap, sizeof(double4) * G, "occulter table")) return s;
+    if (int s = ensure(p->occ32, p->occ32_cap, sizeof(float4) * G, "occulter table")) return s;
     VISS_CUDA(cudaMemcpyAsync(p->occ, occ, sizeof(double4) * G, cudaMemcpyDeviceToDevice, st),
               "viss_plan_set_samples: occulters");
+    VISS_CUDA(viss::launch_occ32(G, p->occ, p->occ32, st), "viss_plan_set_samples: occulters");
   }
   VISS_CUDA(cudaMemsetAsync(p->dev_words + 3, 0, sizeof(unsigned long long), st),
             "viss_plan_set_samples");
@@ -404,6 +408,7 @@ static int forward_impl(viss_plan *p, const float *sky, float *V, int flags, cud
   fp.samp = p->samp;
   fp.refs = masked ? p->refs : nullptr;
   fp.occ = masked ? p->occ : nullptr;
+  fp.occ32 = masked ? p->occ32 : nullptr;
   fp.pix = p->pixsky;
   fp.cones = p->cones;
   fp.K = p->K;
@@ -456,6 +461,7 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
   ap.coef = p->coef;
   ap.refs = masked ? p->refs : nullptr;
   ap.occ = masked ? p->occ : nullptr;
+  ap.occ32 = masked ? p->occ32 : nullptr;
   ap.pix = p->pix;
   ap.cones = p->cones;
   ap.K = p->K;

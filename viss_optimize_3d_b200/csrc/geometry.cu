@@ -119,36 +119,91 @@ __global__ void k_stage_pixels(long long J, long long Jpad, const double *lmn, c
   pix[i] = make_double4(lmn[3 * s], lmn[3 * s + 1], lmn[3 * s + 2], 0.0);
 }
 
-// Bounding cone of each kTilePix-pixel tile: centre = normalised mean,
-// radius = max chord |s - c| plus a relative margin.  One warp per tile.
-__global__ void k_tile_cones(long long ntiles, const double4 *pix, double4 *cones) {
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// FP32 centre of a pixel set with coordinate sums (sx, sy, sz): the
+// normalised mean rounded to float, or (1, 0, 0) when the mean is ~0.
+__device__ __forceinline__ float4 cone_centre(double sx, double sy, double sz, bool &degenerate) {
+  const double nrm = sqrt(sx * sx + sy * sy + sz * sz);
+  degenerate = !(nrm > 1e-6);
+  if (degenerate) return make_float4(1.f, 0.f, 0.f, 0.f);
+  return make_float4(__double2float_rn(sx / nrm), __double2float_rn(sy / nrm),
+                     __double2float_rn(sz / nrm), 0.f);
+}
+
+__device__ __forceinline__ double chord(double x, double y, double z, const float4 &c) {
+  const double dx = x - c.x, dy = y - c.y, dz = z - c.z;
+  return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+// Radius field of an FP32 cone (see cone_state32): the largest chord to the
+// rounded centre plus kConeMargin32, rounded up; 4 (wider than any chord of
+// unit vectors) for a degenerate set, NaN if any pixel is NaN so that every
+// classification falls through to the exact per-pixel test.
+__device__ __forceinline__ float cone_radius(double rho, bool degenerate, bool any_nan) {
+  if (any_nan) return __int_as_float(0x7fc00000);
+  if (degenerate) return 4.f;
+  return __double2float_ru(rho + kConeMargin32);
+}
+
+// FP32 bounding cones: cones[t] for each kTilePix-pixel tile t and
+// cones[ntiles + 4 t + s] for its four 32-pixel sub-tiles (pixels
+// 128 t + 32 s .. + 31).  One warp per tile; lane l holds pixels 32 s + l.
+__global__ void k_tile_cones(long long ntiles, const double4 *pix, float4 *cones) {
   const long long t = static_cast<long long>(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
   if (t >= ntiles) return;
-  double sx = 0, sy = 0, sz = 0;
-  for (int p = lane; p < kTilePix; p += 32) {
-    const double4 q = pix[t * kTilePix + p];
-    sx += q.x; sy += q.y; sz += q.z;
+  double px[4], py[4], pz[4];
+  bool nan_lane = false;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const double4 q = pix[t * kTilePix + 32 * s + lane];
+    px[s] = q.x; py[s] = q.y; pz[s] = q.z;
+    nan_lane = nan_lane || isnan(q.x) || isnan(q.y) || isnan(q.z);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    sx += __shfl_xor_sync(0xffffffffu, sx, o);
-    sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+  double tx = 0, ty = 0, tz = 0;
+  float4 sub[4];
+  bool sub_deg[4], sub_nan[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const double sx = warp_sum(px[s]), sy = warp_sum(py[s]), sz = warp_sum(pz[s]);
+    tx += sx; ty += sy; tz += sz;
+    sub[s] = cone_centre(sx, sy, sz, sub_deg[s]);
+    sub_nan[s] = __any_sync(0xffffffffu, isnan(px[s]) || isnan(py[s]) || isnan(pz[s]));
   }
-  const double nrm = sqrt(sx * sx + sy * sy + sz * sz);
-  double cx = 1, cy = 0, cz = 0;
-  if (nrm > 1e-6) { cx = sx / nrm; cy = sy / nrm; cz = sz / nrm; }
-  double rho = 0;
-  for (int p = lane; p < kTilePix; p += 32) {
-    const double4 q = pix[t * kTilePix + p];
-    const double dx = q.x - cx, dy = q.y - cy, dz = q.z - cz;
-    rho = fmax(rho, sqrt(dx * dx + dy * dy + dz * dz));
+  bool tile_deg;
+  float4 tile = cone_centre(tx, ty, tz, tile_deg);
+  double rho_t = 0;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const double rs = warp_max(chord(px[s], py[s], pz[s], sub[s]));
+    sub[s].w = cone_radius(rs, sub_deg[s], sub_nan[s]);
+    rho_t = fmax(rho_t, chord(px[s], py[s], pz[s], tile));
   }
-  for (int o = 16; o > 0; o >>= 1) rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
-  if (lane == 0) {
-    if (nrm <= 1e-6) rho = 4.0;  // degenerate tile: always "test every pixel"
-    cones[t] = make_double4(cx, cy, cz, rho * (1.0 + 1e-9) + 1e-12);
-  }
+  rho_t = warp_max(rho_t);
+  tile.w = cone_radius(rho_t, tile_deg, __any_sync(0xffffffffu, nan_lane));
+  if (lane < 4) cones[ntiles + 4 * t + lane] = sub[lane];
+  if (lane == 0) cones[t] = tile;
+}
+
+// FP32 occulter rows for the classification: (q, thr) / |q| (the same
+// half-space with a unit direction); rows with |q| = 0 or non-finite |q| are
+// rounded as they are (NaN stays NaN: "test every pixel").
+__global__ void k_occ32(long long G, const double4 *occ, float4 *out) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= G) return;
+  const double4 q = occ[i];
+  const double n = sqrt(q.x * q.x + q.y * q.y + q.z * q.z);
+  const double s = (n > 0.0 && n <= 1.7e308) ? 1.0 / n : 1.0;
+  out[i] = make_float4(__double2float_rn(q.x * s), __double2float_rn(q.y * s),
+                       __double2float_rn(q.z * s), __double2float_rn(q.w * s));
 }
 
 // Sky staging: pixel record + sky value in the low word of .w (zero past J),
@@ -220,12 +275,18 @@ cudaError_t launch_pix_keys(long long J, const double *lmn, unsigned long long *
 }
 
 cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, const int *perm,
-                                double4 *pix, double4 *cones, cudaStream_t st) {
+                                double4 *pix, float4 *cones, cudaStream_t st) {
   k_stage_pixels<<<nblk(Jpad, 256), 256, 0, st>>>(J, Jpad, lmn, perm, pix);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const long long nt = Jpad / kTilePix;
   k_tile_cones<<<nblk(nt, 8), 256, 0, st>>>(nt, pix, cones);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_occ32(long long G, const double4 *occ, float4 *out, cudaStream_t st) {
+  if (G <= 0) return cudaSuccess;
+  k_occ32<<<nblk(G, 256), 256, 0, st>>>(G, occ, out);
   return cudaGetLastError();
 }
 
@@ -281,7 +342,7 @@ cudaError_t sort_pixel_keys(long long J, unsigned long long *keys_in, unsigned l
 
 // Tile cones of already-staged pixel records (used by the allocation-free
 // forward entry point, which stages pixels in the caller's order).
-cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, double4 *cones, cudaStream_t st) {
+cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, float4 *cones, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   k_tile_cones<<<nblk(ntiles, 8), 256, 0, st>>>(ntiles, pix, cones);
   return cudaGetLastError();

@@ -7,13 +7,13 @@
 // through its own pool allocator, or an observation pipeline that must not
 // allocate after start-up.  viss_forward_noalloc computes the same
 // visibilities with every intermediate buffer carved out of one file-scope
-// __device__ array of fixed size (kScratchBytes, 7.5 MiB).  That array exists
+// __device__ array of fixed size (kScratchBytes, about 9 MiB).  That array exists
 // on every GPU that loads the library, for the life of the process, whether
 // or not this entry point is ever called.
 //
 // Limits and rules (also in include/viss.h):
-//   - at most kNaMaxPix pixels and kNaMaxSamp samples per call; larger inputs
-//     are rejected with VISS_ERR_ARG;
+//   - at most kNaMaxPix pixels, kNaMaxSamp samples and kNaMaxOcc occulter
+//     rows per call; larger inputs are rejected with VISS_ERR_ARG;
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current);
 //     make that first call before any stream capture;
@@ -38,8 +38,9 @@
 namespace viss {
 cudaError_t launch_stage_samples(long long, const double *, const double *, const int32_t *,
                                  double4 *, int4 *, unsigned long long *, cudaStream_t);
-cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, double4 *cones,
+cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, float4 *cones,
                               cudaStream_t st);
+cudaError_t launch_occ32(long long G, const double4 *occ, float4 *out, cudaStream_t st);
 int record_error(int status, const std::string &msg);
 }  // namespace viss
 
@@ -47,12 +48,14 @@ namespace {
 
 constexpr long long kNaMaxPix = 65536;   // pixels per call (Nside 64 is 49,152)
 constexpr long long kNaMaxSamp = 32768;  // samples per call
+constexpr long long kNaMaxOcc = 3 * kNaMaxSamp;  // occulter rows per call
 constexpr int kNaMaxChunks = 8;          // cross-block partial sums per sample
 
 // Byte offsets of the regions inside the array (each a multiple of 256).
 constexpr size_t kOffPix = 0;                                        // double4[kNaMaxPix]
-constexpr size_t kOffCones = kOffPix + 32ull * kNaMaxPix;            // double4[kNaMaxPix/128]
-constexpr size_t kOffSamp = kOffCones + 32ull * (kNaMaxPix / viss::kTilePix);  // double4[kNaMaxSamp]
+constexpr size_t kOffCones = kOffPix + 32ull * kNaMaxPix;            // float4[5 * kNaMaxPix/128]
+constexpr size_t kOffOcc32 = kOffCones + 16ull * 5 * (kNaMaxPix / viss::kTilePix);  // float4[kNaMaxOcc]
+constexpr size_t kOffSamp = kOffOcc32 + 16ull * kNaMaxOcc;           // double4[kNaMaxSamp]
 constexpr size_t kOffRefs = kOffSamp + 32ull * kNaMaxSamp;           // int4[kNaMaxSamp]
 constexpr size_t kOffPart = kOffRefs + 16ull * kNaMaxSamp;           // double2[chunks][kNaMaxSamp]
 constexpr size_t kOffWords = kOffPart + 16ull * kNaMaxChunks * kNaMaxSamp;  // 4 x uint64
@@ -126,6 +129,10 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
                           " samples); use viss_forward with a plan");
   if (refs && (G < 1 || !occ))
     return viss::record_error(VISS_ERR_ARG, "viss_forward_noalloc: refs need an occulter table");
+  if (refs && G > kNaMaxOcc)
+    return viss::record_error(VISS_ERR_ARG, "viss_forward_noalloc: " + std::to_string(G) +
+                                                " occulter rows exceeds the fixed scratch (at most " +
+                                                std::to_string(kNaMaxOcc) + "); use viss_forward with a plan");
   if (refs && reinterpret_cast<uintptr_t>(occ) % 16)
     return viss::record_error(VISS_ERR_ARG, "viss_forward_noalloc: occ must be 16-byte aligned");
 
@@ -133,7 +140,8 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   if (int s = na_scratch(&base)) return s;
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   double4 *pix = reinterpret_cast<double4 *>(base + kOffPix);
-  double4 *cones = reinterpret_cast<double4 *>(base + kOffCones);
+  float4 *cones = reinterpret_cast<float4 *>(base + kOffCones);
+  float4 *occ32 = reinterpret_cast<float4 *>(base + kOffOcc32);
   double4 *samp = reinterpret_cast<double4 *>(base + kOffSamp);
   int4 *ref4 = reinterpret_cast<int4 *>(base + kOffRefs);
   double2 *part = reinterpret_cast<double2 *>(base + kOffPart);
@@ -150,6 +158,8 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   k_na_stage_pix<<<static_cast<unsigned>((Jpad + 255) / 256), 256, 0, st>>>(J, Jpad, lmn, sky, pix);
   if ((e = cudaGetLastError()) != cudaSuccess) return na_cuda(e, "stage pixels");
   if ((e = viss::launch_tile_cones(ntiles, pix, cones, st)) != cudaSuccess) return na_cuda(e, "cones");
+  if (refs && (e = viss::launch_occ32(G, reinterpret_cast<const double4 *>(occ), occ32, st)) != cudaSuccess)
+    return na_cuda(e, "occulters");
   if ((e = viss::launch_stage_samples(K, uvw, off, refs, samp, refs ? ref4 : nullptr, words + 3,
                                       st)) != cudaSuccess)
     return na_cuda(e, "stage samples");
@@ -182,6 +192,7 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   fp.samp = samp;
   fp.refs = refs ? ref4 : nullptr;
   fp.occ = refs ? reinterpret_cast<const double4 *>(occ) : nullptr;
+  fp.occ32 = refs ? occ32 : nullptr;
   fp.pix = pix;
   fp.cones = cones;
   fp.K = K;

@@ -14,7 +14,7 @@
 // Work decomposition
 //   forward: a CTA owns NT*R samples (R per thread, in registers) and one
 //            chunk of pixel tiles; tiles of kTilePix pixel records stream
-//            through a 2-deep shared-memory ring filled by cp.async.bulk
+//            through a 3-stage shared-memory ring filled by cp.async.bulk
 //            (TMA engine) and are read as warp-wide broadcasts.  Partial sums
 //            of each chunk go to a [chunk][K] FP64 workspace; k_reduce_fwd
 //            adds the chunks in FP64.
@@ -53,14 +53,14 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
 // Classification of a sample (3 occulter refs) against one tile cone, packed:
 // bits 0-1 state (2 every pixel visible, 0 none, 1 mixed), bits 2-4 which
 // refs are mixed on this tile (only those need the per-pixel test).
-__device__ __forceinline__ int sample_state(const int4 &rf, const double4 &cone,
-                                            const double4 *occ) {
+__device__ __forceinline__ int sample_state(const int4 &rf, const float4 &cone,
+                                            const float4 *occ32) {
   int st = 2, need = 0;
   const int r3[3] = {rf.x, rf.y, rf.z};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (r3[c] < 0) continue;
-    const int s = cone_state(cone, occ[r3[c]]);
+    const int s = cone_state32(cone, occ32[r3[c]]);
     st = min(st, s);
     if (s == 1) need |= 1 << c;
   }
@@ -70,9 +70,9 @@ __device__ __forceinline__ int sample_state(const int4 &rf, const double4 &cone,
 // The same against the union of two tiles (a warp tile of 256 pixels): hidden
 // only if hidden on both; all visible only if all visible on both; otherwise
 // every ref that is not all-visible on both tiles is tested per pixel.
-__device__ __forceinline__ int sample_state2(const int4 &rf, const double4 &c0,
-                                             const double4 &c1, const double4 *occ) {
-  const int a = sample_state(rf, c0, occ), b = sample_state(rf, c1, occ);
+__device__ __forceinline__ int sample_state2(const int4 &rf, const float4 &c0, const float4 &c1,
+                                             const float4 *occ32) {
+  const int a = sample_state(rf, c0, occ32), b = sample_state(rf, c1, occ32);
   const int sa = a & 3, sb = b & 3;
   if (sa == 0 && sb == 0) return 0;
   if (sa == 2 && sb == 2) return 2;
@@ -88,20 +88,75 @@ __device__ __forceinline__ int sample_state2(const int4 &rf, const double4 &c0,
   return need ? (1 | (need << 2)) : 2;
 }
 
-// The occulter rows a mixed sample must test; rows it need not test become a
-// row every direction passes (thr = -4 < any dot of unit vectors).
-__device__ __forceinline__ void mixed_rows(const int4 &rf, int code, const double4 *occ,
-                                           double4 &q0, double4 &q1, double4 &q2) {
-  const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
-  q0 = (code & 4) ? occ[rf.x] : pass;
-  q1 = (code & 8) ? occ[rf.y] : pass;
-  q2 = (code & 16) ? occ[rf.z] : pass;
+// The occulter rows a mixed sample must test (need bits 2-4 of its state
+// code), compacted to the front: their indices (-1 past the count) and the
+// count.
+__device__ __forceinline__ int needed_idx(const int4 &rf, int code, int &i0, int &i1, int &i2) {
+  i0 = i1 = i2 = -1;
+  if (code & 4) i0 = rf.x;
+  if (code & 8) {
+    if (i0 < 0) i0 = rf.y;
+    else i1 = rf.y;
+  }
+  if (code & 16) {
+    if (i0 < 0) i0 = rf.z;
+    else if (i1 < 0) i1 = rf.z;
+    else i2 = rf.z;
+  }
+  return (i0 >= 0) + (i1 >= 0) + (i2 >= 0);
 }
 
+// Exact rows for those indices; absent rows pass every direction (thr = -4
+// is below any dot product of unit vectors).
+__device__ __forceinline__ void exact_rows(const double4 *occ, int i0, int i1, int i2,
+                                           double4 &q0, double4 &q1, double4 &q2) {
+  const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
+  q0 = i0 >= 0 ? occ[i0] : pass;
+  q1 = i1 >= 0 ? occ[i1] : pass;
+  q2 = i2 >= 0 ? occ[i2] : pass;
+}
+
+// Classification rows for those indices.
+__device__ __forceinline__ void class_rows(const float4 *occ32, int i0, int i1, int i2,
+                                           float4 &f0, float4 &f1, float4 &f2) {
+  const float4 pass32 = make_float4(0.f, 0.f, 0.f, -4.f);
+  f0 = i0 >= 0 ? occ32[i0] : pass32;
+  f1 = i1 >= 0 ? occ32[i1] : pass32;
+  f2 = i2 >= 0 ? occ32[i2] : pass32;
+}
+
+// Both, for one sample; returns how many rows need the test.
+__device__ __forceinline__ int needed_rows(const int4 &rf, int code, const double4 *occ,
+                                           const float4 *occ32, double4 &q0, double4 &q1,
+                                           double4 &q2, float4 &f0, float4 &f1, float4 &f2) {
+  int i0, i1, i2;
+  const int n = needed_idx(rf, code, i0, i1, i2);
+  exact_rows(occ, i0, i1, i2, q0, q1, q2);
+  class_rows(occ32, i0, i1, i2, f0, f1, f2);
+  return n;
+}
+
+// State of one cone against the first n classification rows (2 visible, 0
+// hidden, 1 mixed).
+__device__ __forceinline__ int rows_state(const float4 &cone, int n, const float4 &f0,
+                                          const float4 &f1, const float4 &f2) {
+  int st = 2;
+  if (n > 0) st = min(st, cone_state32(cone, f0));
+  if (n > 1) st = min(st, cone_state32(cone, f1));
+  if (n > 2) st = min(st, cone_state32(cone, f2));
+  return st;
+}
+
+// Exact visibility of direction s against the first NROWS rows (the same IEEE
+// operations as the CPU oracle's predicate).
+template <int NROWS>
 __device__ __forceinline__ bool visible_rows(const double4 &q0, const double4 &q1,
                                              const double4 &q2, double s0, double s1, double s2) {
-  return (dot_exact(s0, s1, s2, q0) >= q0.w) & (dot_exact(s0, s1, s2, q1) >= q1.w) &
-         (dot_exact(s0, s1, s2, q2) >= q2.w);
+  bool v = true;
+  if (NROWS > 0) v = dot_exact(s0, s1, s2, q0) >= q0.w;
+  if (NROWS > 1) v = v & (dot_exact(s0, s1, s2, q1) >= q1.w);
+  if (NROWS > 2) v = v & (dot_exact(s0, s1, s2, q2) >= q2.w);
+  return v;
 }
 
 __device__ __forceinline__ float sky_of(const double4 &p) {
@@ -134,15 +189,44 @@ __device__ __forceinline__ void fwd_term(double t, float I, float &re, float &im
 // ======================================================================
 // forward
 // ======================================================================
+// Pixels per forward sub-tile (the span a mixed sample row is refined to).
+constexpr int kSubPix = 32;
+
+// One sample over kSubPix staged records, in pairs (even record at mk, odd
+// record half a turn on at mk2 and negated), testing the first NROWS
+// occulter rows per term (NROWS = 0: every pixel visible).
+template <int NROWS, bool FP64>
+__device__ __forceinline__ void fwd_span(const double4 *tp, double ux, double uy, double uz,
+                                         double mk, double mk2, const double4 &q0,
+                                         const double4 &q1, const double4 &q2, float &re,
+                                         float &im, double &dre, double &dim) {
+#pragma unroll 2
+  for (int j = 0; j < kSubPix; j += 2) {
+    const double4 a = tp[j], b = tp[j + 1];
+    float Ia = sky_of(a), Ib = FP64 ? sky_of(b) : -sky_of(b);
+    if (NROWS > 0) {
+      Ia = visible_rows<NROWS>(q0, q1, q2, a.x, a.y, a.z) ? Ia : 0.f;
+      Ib = visible_rows<NROWS>(q0, q1, q2, b.x, b.y, b.z) ? Ib : 0.f;
+    }
+    const double ta = fma(uz, a.z, fma(uy, a.y, fma(ux, a.x, mk)));
+    fwd_term<FP64>(ta, Ia, re, im, dre, dim);
+    const double tb = fma(uz, b.z, fma(uy, b.y, fma(ux, b.x, mk2)));
+    fwd_term<FP64>(tb, Ib, re, im, dre, dim);
+  }
+}
+
 template <int NT, int R, int MINB, bool MASKED, bool FP64>
 __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
-  __shared__ __align__(128) double4 s_pix[2][kTilePix];
+  constexpr int S = kFwdStages;
+  constexpr int kWarps = NT / 32;
+  __shared__ __align__(128) double4 s_pix[S][kTilePix];
   __shared__ __align__(16) int4 s_refs[MASKED ? R : 1][MASKED ? NT : 1];
   // Kahan (sum, comp) of re and im per sample, kept in shared memory (touched
   // once per tile) so the registers hold only what the inner loop needs
   __shared__ float s_kahan[FP64 ? 1 : 4][FP64 ? 1 : R][FP64 ? 1 : NT];
-  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ __align__(8) uint64_t s_full[S], s_empty[S];
   __shared__ int s_abort;
+  volatile int *abort_flag = &s_abort;
 
   const int tid = threadIdx.x;
   // CTAs never straddle channels: blockIdx.x = channel * blocks_per_channel + block
@@ -178,43 +262,46 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   }
 
   const int t0 = blockIdx.y * p.tiles_per_chunk;
-  const int t1 = min(t0 + p.tiles_per_chunk, p.ntiles);
+  const int ntile = max(0, min(t0 + p.tiles_per_chunk, p.ntiles) - t0);
   constexpr uint32_t kTileBytes = kTilePix * sizeof(double4);
+  auto issue = [&](int i, int stage) {
+    mbar_expect_tx(&s_full[stage], kTileBytes);
+    bulk_g2s(s_pix[stage], pix + static_cast<long long>(t0 + i) * kTilePix, kTileBytes,
+             &s_full[stage]);
+  };
 
   if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&s_full[s], 1);
+      mbar_init(&s_empty[s], kWarps);
+    }
     fence_mbar_init();
     s_abort = 0;
   }
   __syncthreads();
-  if (tid == 0 && t0 < t1) {
-    mbar_expect_tx(&s_bar[0], kTileBytes);
-    bulk_g2s(s_pix[0], pix + static_cast<long long>(t0) * kTilePix, kTileBytes, &s_bar[0]);
-  }
 
   unsigned long long evaluated = 0, mixed_terms = 0;
-  int it = 0;
-  for (int t = t0; t < t1; ++t, ++it) {
-    const int buf = it & 1;
-    const uint32_t par = (it >> 1) & 1;
-    if (tid == 0 && t + 1 < t1) {
-      mbar_expect_tx(&s_bar[buf ^ 1], kTileBytes);
-      bulk_g2s(s_pix[buf ^ 1], pix + static_cast<long long>(t + 1) * kTilePix, kTileBytes,
-               &s_bar[buf ^ 1]);
+  int next = 0;  // next tile to issue (producer state, thread 0)
+  for (int it = 0; it < ntile; ++it) {
+    const int t = t0 + it, stage = it % S;
+    if (tid == 0 && !ring_refill<S>(s_empty, next, it, ntile, issue)) {
+      atomicOr(p.err, kErrTimeout);
+      *abort_flag = 1;
     }
+    if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
     // classify the tile for this warp's samples
     int mode = 2;
     int st[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) st[r] = 2;
     if (MASKED) {
-      const double4 cone = p.cones[t];
+      const float4 cone = p.cones[t];
       bool full = true, any = false;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if (kval[r]) {
-          st[r] = sample_state(s_refs[r][tid], cone, p.occ);
+          st[r] = sample_state(s_refs[r][tid], cone, p.occ32);
           full = full && (st[r] == 2);
           any = any || ((st[r] & 3) != 0);
         }
@@ -223,21 +310,19 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
       const bool wany = __any_sync(0xffffffffu, any);
       mode = wfull ? 2 : (wany ? 1 : 0);
     }
-    if (!mbar_wait_bounded(&s_bar[buf], par)) {
-      atomicOr(p.err, kErrTimeout);
-      s_abort = 1;
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_full[stage], static_cast<uint32_t>(it / S) & 1u))) {
+      if ((tid & 31) == 0) atomicOr(p.err, kErrTimeout);
+      *abort_flag = 1;
+      break;
     }
-    const double4 *tp = s_pix[buf];
+    const double4 *tp = s_pix[stage];
     if (mode != 0) {
-      if ((tid & 31) == 0) {
-        evaluated += static_cast<unsigned long long>(nval_warp) * kTilePix;
-        if (mode == 1) mixed_terms += static_cast<unsigned long long>(nval_warp) * kTilePix;
-      }
       float t_re[R], t_im[R];
       double e_re[R], e_im[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) { t_re[r] = t_im[r] = 0.f; e_re[r] = e_im[r] = 0.0; }
       if (mode == 2) {
+        if ((tid & 31) == 0) evaluated += static_cast<unsigned long long>(nval_warp) * kTilePix;
         for (int j = 0; j < kTilePix; j += 2) {
           const double4 q0 = tp[j], q1 = tp[j + 1];
           const float I0 = sky_of(q0);
@@ -251,28 +336,47 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
           }
         }
       } else {
-        // mixed tile: one sample at a time, its occulter rows in registers
+        // mixed tile: one sample row at a time.  A lane whose sample needs
+        // the per-term test classifies it against the tile's four 32-pixel
+        // sub-tile cones; the warp then runs each sub-tile once, with the
+        // exact test of as many occulter rows as its neediest lane has there
+        // (lanes that see all of the sub-tile pass every test by
+        // construction), or without a test, and skips a sub-tile no lane
+        // sees.  Lanes that see none of a sub-tile sit it out.
+        const float4 *sub = p.cones + p.ntiles + 4LL * t;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if ((st[r] & 3) == 0) continue;
-          if (st[r] == 2) {
-            for (int j = 0; j < kTilePix; ++j) {
-              const double4 q = tp[j];
-              const bool odd = !FP64 && (j & 1);
-              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, odd ? mk2[r] : mk[r])));
-              fwd_term<FP64>(t, odd ? -sky_of(q) : sky_of(q), t_re[r], t_im[r], e_re[r], e_im[r]);
+          const int code = kval[r] ? st[r] : 0;
+          double4 q0, q1, q2;
+          float4 f0, f1, f2;
+          const int nr = needed_rows(s_refs[r][tid], (code & 3) == 1 ? code : 0, p.occ, p.occ32,
+                                     q0, q1, q2, f0, f1, f2);
+          // 2 bits per sub-tile: 2 all visible, 0 none, 1 test per pixel
+          unsigned ss = (code & 3) == 2 ? 0xAAu : 0u;
+          if ((code & 3) == 1) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b) ss |= static_cast<unsigned>(rows_state(sub[b], nr, f0, f1, f2)) << (2 * b);
+          }
+#pragma unroll 1
+          for (int b = 0; b < 4; ++b) {
+            const unsigned sst = (ss >> (2 * b)) & 3u;
+            const unsigned seen = __ballot_sync(0xffffffffu, sst != 0);
+            if (seen == 0) continue;
+            const int wn = __reduce_max_sync(0xffffffffu, sst == 1 ? nr : 0);
+            if ((tid & 31) == 0) {
+              evaluated += static_cast<unsigned long long>(__popc(seen)) * kSubPix;
+              if (wn) mixed_terms += static_cast<unsigned long long>(__popc(seen)) * kSubPix;
             }
-          } else {
-            double4 q0, q1, q2;
-            mixed_rows(s_refs[r][tid], st[r], p.occ, q0, q1, q2);
-            for (int j = 0; j < kTilePix; ++j) {
-              const double4 q = tp[j];
-              const bool odd = !FP64 && (j & 1);
-              float Iv = visible_rows(q0, q1, q2, q.x, q.y, q.z) ? sky_of(q) : 0.f;
-              if (odd) Iv = -Iv;
-              const double t = fma(uz[r], q.z, fma(uy[r], q.y, fma(ux[r], q.x, odd ? mk2[r] : mk[r])));
-              fwd_term<FP64>(t, Iv, t_re[r], t_im[r], e_re[r], e_im[r]);
-            }
+            if (sst == 0) continue;
+            const double4 *sp = tp + b * kSubPix;
+            if (wn == 0)
+              fwd_span<0, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
+            else if (wn == 1)
+              fwd_span<1, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
+            else if (wn == 2)
+              fwd_span<2, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
+            else
+              fwd_span<3, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
           }
         }
       }
@@ -291,13 +395,9 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
         }
       }
     }
-    __syncthreads();  // every warp is done with buf before it is refilled
-    if (s_abort) {
-      // a copy was lost: let the other buffer's copy (if any) land, bounded
-      if (tid == 0 && t + 1 < t1) mbar_wait_bounded(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
-      break;
-    }
+    ring_release(s_empty, stage);
   }
+  if (tid == 0) ring_drain<S>(s_full, next);
 
   if (p.counter && (tid & 31) == 0) {
     if (evaluated) atomicAdd(p.counter, evaluated);
@@ -342,33 +442,33 @@ __global__ void k_reduce_fwd(long long K, int nchunk, const double2 *part, float
 // ======================================================================
 // adjoint
 // ======================================================================
-template <int P, bool MIXED, bool FP64>
+// One sample into a lane's P pixels (pixel q of every lane lies in the warp's
+// 32-pixel sub-tile q).  Bit q of the warp-uniform `hid` zeroes sub-tile q
+// (none of it visible); NROWS > 0 tests the first NROWS occulter rows on
+// every term.  The P terms stay one branch-free block: splitting them by
+// sub-tile would serialise their DFMA -> MUFU latency chains, which costs more
+// than evaluating a hidden term.
+template <int P, int NROWS, bool FP64>
 __device__ __forceinline__ void adj_sample(const double4 &u, double m, const float2 &a,
                                            const double (&sx)[P], const double (&sy)[P],
                                            const double (&sz)[P], const double4 &q0,
-                                           const double4 &q1, const double4 &q2, float (&acc)[P],
-                                           double (&dacc)[P]) {
+                                           const double4 &q1, const double4 &q2, unsigned hid,
+                                           float (&acc)[P], double (&dacc)[P]) {
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     const double t = fma(u.z, sz[q], fma(u.y, sy[q], fma(u.x, sx[q], m)));
-    bool vis = true;
-    if (MIXED) vis = visible_rows(q0, q1, q2, sx[q], sy[q], sz[q]);
+    bool vis = ((hid >> q) & 1u) == 0;
+    if (NROWS > 0) vis = vis & visible_rows<NROWS>(q0, q1, q2, sx[q], sy[q], sz[q]);
+    const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
     if (FP64) {
       double sn, cs;
       sincos_turns_fp64(t, sn, cs);
-      const double c = fma(static_cast<double>(a.x), cs, -static_cast<double>(a.y) * sn);
-      dacc[q] += vis ? c : 0.0;
+      dacc[q] += fma(static_cast<double>(ar), cs, -static_cast<double>(ai) * sn);
     } else {
       float sn, cs;
       sfu_sincos(turn_angle(t), sn, cs);
-      if (MIXED) {
-        const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
-        acc[q] = fmaf(ar, cs, acc[q]);
-        acc[q] = fmaf(-ai, sn, acc[q]);
-      } else {
-        acc[q] = fmaf(a.x, cs, acc[q]);
-        acc[q] = fmaf(-a.y, sn, acc[q]);
-      }
+      acc[q] = fmaf(ar, cs, acc[q]);
+      acc[q] = fmaf(-ai, sn, acc[q]);
     }
   }
 }
@@ -378,14 +478,18 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   static_assert(P == 4 || P == 8, "a warp covers one or two pixel tiles");
   constexpr int kWarpPix = 32 * P;
   __shared__ float s_kahan[FP64 ? 1 : 2][FP64 ? 1 : P][FP64 ? 1 : NT];  // (sum, comp) per pixel
-  __shared__ __align__(128) double4 s_samp[2][kSampTile];
-  __shared__ __align__(16) float2 s_coef[2][kSampTile];
-  __shared__ __align__(16) int4 s_refs[MASKED ? 2 : 1][MASKED ? kSampTile : 1];
-  __shared__ __align__(8) uint64_t s_bar[2];
+  constexpr int S = kAdjStages;
+  __shared__ __align__(128) double4 s_samp[S][kSampTile];
+  __shared__ __align__(16) float2 s_coef[S][kSampTile];
+  __shared__ __align__(16) int4 s_refs[MASKED ? S : 1][MASKED ? kSampTile : 1];
+  __shared__ __align__(8) uint64_t s_full[S], s_empty[S];
   __shared__ int s_abort;
+  volatile int *abort_flag = &s_abort;
+  constexpr int kWarps = NT / 32;
+  // each warp's P sub-tile cones (sub-tile q = pixels pbase + 32 q .. + 31)
+  __shared__ float4 s_sub[MASKED ? kWarps : 1][MASKED ? P : 1];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int kWarps = NT / 32;
   const long long wtile = static_cast<long long>(blockIdx.x) * kWarps + warp;
   const long long pbase = wtile * kWarpPix;
   const bool tile_ok = pbase < p.Jpad;
@@ -397,11 +501,15 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
     const double4 v = tile_ok ? p.pix[j] : make_double4(0, 0, 1, 0);
     sx[q] = v.x; sy[q] = v.y; sz[q] = v.z;
   }
-  double4 cone0 = make_double4(0, 0, 1, 4.0), cone1 = cone0;
+  // the warp's tile cone(s) in registers, its sub-tile cones in shared memory
+  float4 cone0 = make_float4(0.f, 0.f, 1.f, 4.f), cone1 = cone0;
   if (MASKED && tile_ok) {
+    const long long ntiles = p.Jpad / kTilePix;
     cone0 = p.cones[pbase / kTilePix];
     if (P == 8) cone1 = p.cones[pbase / kTilePix + 1];
+    if (lane < P) s_sub[warp][lane] = p.cones[ntiles + pbase / 32 + lane];
   }
+  __syncwarp();
 
   double dacc[P];
 #pragma unroll
@@ -416,26 +524,29 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   const long long k1 = min(k0 + p.samples_per_chunk, (ch + 1) * p.Kc);
   const int ntile = static_cast<int>((k1 - k0 + kSampTile - 1) / kSampTile);
 
-  auto issue = [&](int it, int buf) {
-    const long long kk = k0 + static_cast<long long>(it) * kSampTile;
+  auto issue = [&](int i, int stage) {
+    const long long kk = k0 + static_cast<long long>(i) * kSampTile;
     const int n = static_cast<int>(min(static_cast<long long>(kSampTile), k1 - kk));
     // sizes in multiples of 16 B: samp 32 B each, coef 8 B each (pad to even), refs 16 B
     const int nc = (n + 1) & ~1;
     uint32_t bytes = n * 32u + nc * 8u + (MASKED ? n * 16u : 0u);
-    mbar_expect_tx(&s_bar[buf], bytes);
-    bulk_g2s(s_samp[buf], p.samp + kk, n * 32u, &s_bar[buf]);
-    bulk_g2s(s_coef[buf], p.coef + kk, nc * 8u, &s_bar[buf]);
-    if (MASKED) bulk_g2s(s_refs[buf], p.refs + kk, n * 16u, &s_bar[buf]);
+    mbar_expect_tx(&s_full[stage], bytes);
+    bulk_g2s(s_samp[stage], p.samp + kk, n * 32u, &s_full[stage]);
+    bulk_g2s(s_coef[stage], p.coef + kk, nc * 8u, &s_full[stage]);
+    if (MASKED) bulk_g2s(s_refs[stage], p.refs + kk, n * 16u, &s_full[stage]);
   };
 
   if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&s_full[s], 1);
+      mbar_init(&s_empty[s], kWarps);
+    }
     fence_mbar_init();
     s_abort = 0;
   }
   __syncthreads();
-  if (tid == 0 && ntile > 0) issue(0, 0);
+  int next = 0;  // next tile to issue (producer state, thread 0)
 
   unsigned long long evaluated = 0, mixed_terms = 0;
   const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
@@ -444,12 +555,16 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   const bool odd_lane = (lane & 1) != 0;
   const double magic = odd_lane ? kMagic + 0.5 : kMagic;
   for (int it = 0; it < ntile; ++it) {
-    const int buf = it & 1;
-    const uint32_t par = (it >> 1) & 1;
-    if (tid == 0 && it + 1 < ntile) issue(it + 1, buf ^ 1);
-    if (!mbar_wait_bounded(&s_bar[buf], par)) {
+    const int buf = it % S;
+    if (tid == 0 && !ring_refill<S>(s_empty, next, it, ntile, issue)) {
       atomicOr(p.err, kErrTimeout);
-      s_abort = 1;
+      *abort_flag = 1;
+    }
+    if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_full[buf], static_cast<uint32_t>(it / S) & 1u))) {
+      if (lane == 0) atomicOr(p.err, kErrTimeout);
+      *abort_flag = 1;
+      break;
     }
     const long long kk = k0 + static_cast<long long>(it) * kSampTile;
     const int n = static_cast<int>(min(static_cast<long long>(kSampTile), k1 - kk));
@@ -462,40 +577,76 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
 #pragma unroll
     for (int q = 0; q < P; ++q) { t_acc[q] = 0.f; e_acc[q] = 0.0; }
     for (int g = 0; g < n; g += 32) {
-      // lane l classifies sample g+l against this warp's pixels
+      // lane l classifies sample g+l against this warp's pixels; a sample
+      // that is mixed on the warp's tile(s) is refined against the P
+      // sub-tile cones: subm = hidden sub-tiles (bits 0-7) | sub-tiles that
+      // need the per-pixel test (bits 8-15)
       const int gn = min(32, n - g);
       int st = (lane < gn) ? 2 : 0;
+      unsigned subm = 0;
       if (MASKED) {
         st = 0;
         if (lane < gn && tile_ok) {
           const int4 rf = s_refs[buf][g + lane];
-          st = (P == 8) ? sample_state2(rf, cone0, cone1, p.occ) : sample_state(rf, cone0, p.occ);
+          st = (P == 8) ? sample_state2(rf, cone0, cone1, p.occ32) : sample_state(rf, cone0, p.occ32);
+          if ((st & 3) == 1) {
+            int i0, i1, i2;
+            const int nr = needed_idx(rf, st, i0, i1, i2);
+            float4 f0, f1, f2;
+            class_rows(p.occ32, i0, i1, i2, f0, f1, f2);
+            unsigned hid = 0, mix = 0;
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+              const int ss = rows_state(s_sub[warp][q], nr, f0, f1, f2);
+              hid |= static_cast<unsigned>(ss == 0) << q;
+              mix |= static_cast<unsigned>(ss == 1) << q;
+            }
+            if (hid == (1u << P) - 1) st = 0;  // hidden on every sub-tile
+            subm = hid | (mix << 8);
+          }
         }
       }
       const unsigned live = __ballot_sync(0xffffffffu, (st & 3) != 0);
       const unsigned mixm = __ballot_sync(0xffffffffu, (st & 3) == 1);
       evaluated += static_cast<unsigned long long>(__popc(live)) * kWarpPix;
-      mixed_terms += static_cast<unsigned long long>(__popc(mixm)) * kWarpPix;
+      if (MASKED && mixm)  // samples that run the per-term test, on all their P sub-tiles
+        mixed_terms += static_cast<unsigned long long>(
+                           __popc(__ballot_sync(0xffffffffu, (st & 3) == 1 && (subm >> 8) != 0))) *
+                       kWarpPix;
       // samples visible on every pixel of the warp: no test, uniform loop
       for (unsigned fast = live & ~mixm; fast; fast &= fast - 1) {
         const int i = __ffs(fast) - 1;
         const double4 u = sp[g + i];
         const float2 a = cp[g + i];
         const double uoff = p.use_off ? u.w : 0.0;
-        adj_sample<P, false, FP64>(u, FP64 ? uoff : magic + uoff, a, sx, sy, sz, pass, pass,
-                                   pass, t_acc, e_acc);
+        adj_sample<P, 0, FP64>(u, FP64 ? uoff : magic + uoff, a, sx, sy, sz, pass, pass, pass,
+                               0u, t_acc, e_acc);
       }
-      // samples that need the per-pixel occultation test
+      // samples mixed on the warp's tiles: hidden sub-tiles zeroed; the exact
+      // per-term test only for samples with a sub-tile that needs it
       for (unsigned mb = mixm; mb; mb &= mb - 1) {
         const int i = __ffs(mb) - 1;
-        const int sst = __shfl_sync(0xffffffffu, st, i);
+        const unsigned sm = __shfl_sync(0xffffffffu, subm, i);
+        const unsigned hid = sm & 0xffu;
         const double4 u = sp[g + i];
         const float2 a = cp[g + i];
         const double uoff = p.use_off ? u.w : 0.0;
+        const double mm = FP64 ? uoff : magic + uoff;
+        if ((sm >> 8) == 0) {
+          adj_sample<P, 0, FP64>(u, mm, a, sx, sy, sz, pass, pass, pass, hid, t_acc, e_acc);
+          continue;
+        }
+        const int sst = __shfl_sync(0xffffffffu, st, i);
+        int i0, i1, i2;
+        const int nr = needed_idx(s_refs[buf][g + i], sst, i0, i1, i2);
         double4 q0, q1, q2;
-        mixed_rows(s_refs[buf][g + i], sst, p.occ, q0, q1, q2);
-        adj_sample<P, true, FP64>(u, FP64 ? uoff : magic + uoff, a, sx, sy, sz, q0, q1, q2,
-                                  t_acc, e_acc);
+        exact_rows(p.occ, i0, i1, i2, q0, q1, q2);
+        if (nr == 1)
+          adj_sample<P, 1, FP64>(u, mm, a, sx, sy, sz, q0, q1, q2, hid, t_acc, e_acc);
+        else if (nr == 2)
+          adj_sample<P, 2, FP64>(u, mm, a, sx, sy, sz, q0, q1, q2, hid, t_acc, e_acc);
+        else
+          adj_sample<P, 3, FP64>(u, mm, a, sx, sy, sz, q0, q1, q2, hid, t_acc, e_acc);
       }
     }
 #pragma unroll
@@ -509,12 +660,9 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
         s_kahan[1][q][tid] = c;
       }
     }
-    __syncthreads();
-    if (s_abort) {
-      if (tid == 0 && it + 1 < ntile) mbar_wait_bounded(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
-      break;
-    }
+    ring_release(s_empty, buf);
   }
+  if (tid == 0) ring_drain<S>(s_full, next);
 
   if (p.counter && lane == 0 && tile_ok) {
     if (evaluated) atomicAdd(p.counter, evaluated);

@@ -7,13 +7,16 @@
 namespace viss {
 
 constexpr int kSampTile = 128;  // samples per adjoint staging tile
+constexpr int kFwdStages = 3;   // shared-memory ring depth: forward pixel tiles
+constexpr int kAdjStages = 4;   // shared-memory ring depth: adjoint sample tiles
 
 struct FwdParams {
   const double4 *samp;   // [K] (u, v, w, off)
   const int4 *refs;      // [K] occulter rows or null
-  const double4 *occ;    // [G]
+  const double4 *occ;    // [G] exact rows
+  const float4 *occ32;   // [G] classification rows
   const double4 *pix;    // [Jpad] (l, m, n, sky bits in the low word)
-  const double4 *cones;  // [ntiles]
+  const float4 *cones;   // [ntiles] tile cones, then [4 * ntiles] sub-tile cones
   long long K;
   int ntiles;
   int tiles_per_chunk;
@@ -30,11 +33,12 @@ struct AdjParams {
   const double4 *samp;   // [K] (u, v, w, off)
   const float2 *coef;    // [Kpad] plan-owned copy, padded to an even count
   const int4 *refs;      // [K] or null
-  const double4 *occ;
+  const double4 *occ;    // [G] exact rows
+  const float4 *occ32;   // [G] classification rows
   const double4 *pix;    // [Jpad] (l, m, n, -)
-  const double4 *cones;  // [ntiles]
+  const float4 *cones;   // [ntiles] tile cones, then [4 * ntiles] sub-tile cones
   long long K;
-  long long Jpad;
+  long long Jpad;         // a multiple of 2 * kTilePix
   int samples_per_chunk;  // multiple of kSampTile
   double *part;           // [nchunk][Jpad]
   unsigned long long *counter;

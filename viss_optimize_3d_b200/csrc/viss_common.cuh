@@ -5,9 +5,10 @@
 //   sky           float                      4 B / pixel (zero in the padding)
 //   sample record double4 (u, v, w, off)     32 B / sample
 //   refs          int4 (ga, gb, ge, -1)      16 B / sample (occulter rows, -1 none)
-//   occulter      double4 (qx, qy, qz, thr)  32 B / occulter
-//   tile cone     double4 (cx, cy, cz, rho)  32 B / pixel tile: every pixel s of
-//                 the tile has |s - c| <= rho
+//   occulter      double4 (qx, qy, qz, thr)  32 B / occulter (exact test)
+//   occulter32    float4 (q, thr) / |q|      16 B / occulter (classification)
+//   cones         float4 (cx, cy, cz, w)     16 B per pixel tile, then 4 x 16 B
+//                 per tile for its 32-pixel sub-tiles (see cone_state32)
 #pragma once
 
 #include <cstdint>
@@ -51,7 +52,13 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                : "memory");
 }
 
-// One-shot try: returns true when the phase with the given parity completed.
+// Arrive (count one) on a barrier without waiting.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// One-shot try: returns true when the phase with the given parity completed
+// (may suspend the thread for a hardware-chosen interval first).
 __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -64,13 +71,40 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: gives up after `limit` polls (each try_wait already suspends
-// for a hardware-chosen interval), so a lost copy ends the kernel with an
-// error flag instead of a hung GPU.
+// Non-blocking test of the same condition.
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait: gives up after `limit_ns` nanoseconds of the global timer (or
+// 2^26 polls, whichever comes first), so a lost copy or a stalled peer warp
+// ends the kernel with an error flag instead of a hung GPU.  The default
+// limit is far above any legitimate wait in these kernels (one tile of work).
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
-                                                  uint32_t limit = (1u << 22)) {
-  for (uint32_t i = 0; i < limit; ++i)
-    if (mbar_try(bar, parity)) return true;
+                                                  uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t start = global_ns();
+  for (uint32_t i = 0; i < (1u << 20); ++i) {
+#pragma unroll 1
+    for (int j = 0; j < 64; ++j)
+      if (mbar_try(bar, parity)) return true;
+    if (global_ns() - start > limit_ns) return false;
+  }
   return false;
 }
 
@@ -83,6 +117,54 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
           "r"(smem_addr(dst_smem)),
       "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
+}
+
+// --------------------------------------------------------------- stage ring
+// An S-stage ring of shared-memory tiles filled by bulk copies.  full[s]
+// (count 1) completes when the tile in stage s has landed; empty[s] (count =
+// the CTA's warps) completes when every warp has released it.  Tile i lives
+// in stage i % S and is phase (i / S) & 1 of both barriers.  One thread (the
+// producer, itself a consumer in warp 0) refills stages as they free up, so
+// warps drift up to S - 1 tiles apart instead of meeting at a CTA barrier
+// after every tile.
+
+// Producer: issue tiles [next, min(ntile, it + S)) in order through
+// issue(i, stage).  A stage still held by a slower warp stops the refill
+// (retried at the producer's next tile) unless it is needed for tile `it`,
+// the one the producer's own warp consumes now, which is waited for
+// (bounded).  Returns false on a timeout.
+template <int S, typename Issue>
+__device__ __forceinline__ bool ring_refill(uint64_t *empty, int &next, int it, int ntile,
+                                            Issue &&issue) {
+  while (next < ntile && next < it + S) {
+    const int s = next % S;
+    if (next >= S) {
+      const uint32_t par = static_cast<uint32_t>(next / S - 1) & 1u;
+      if (next == it) {
+        if (!mbar_wait_bounded(&empty[s], par)) return false;
+      } else if (!mbar_test(&empty[s], par)) {
+        break;
+      }
+    }
+    issue(next, s);
+    ++next;
+  }
+  return true;
+}
+
+// Consumer: the calling warp is done reading stage s.
+__device__ __forceinline__ void ring_release(uint64_t *empty, int s) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[s]);
+}
+
+// Producer, before the CTA exits: let every copy still in flight land, bounded.
+// Tile i is issued only after tile i - S was consumed, so only the last S
+// issued tiles can still be in flight.
+template <int S>
+__device__ __forceinline__ void ring_drain(uint64_t *full, int next) {
+  for (int i = next > S ? next - S : 0; i < next; ++i)
+    mbar_wait_bounded(&full[i % S], static_cast<uint32_t>(i / S) & 1u);
 }
 
 // ------------------------------------------------------------- phase helpers
@@ -111,15 +193,22 @@ __device__ __forceinline__ double dot_exact(double s0, double s1, double s2, con
   return __fma_rn(s2, q.z, __fma_rn(s1, q.y, __dmul_rn(s0, q.x)));
 }
 
-// Tile-vs-occulter classification.  Returns 2 if every pixel of the tile is
-// visible, 0 if none is, 1 if the tile must be tested pixel by pixel.  The
-// bound |s.q - c.q| <= |s - c| <= rho holds for every pixel; kConeEps covers
-// the rounding of the per-pixel dot product and of c.q.
-constexpr double kConeEps = 1e-12;
-__device__ __forceinline__ int cone_state(const double4 &cone, const double4 &q) {
-  const double d = cone.x * q.x + cone.y * q.y + cone.z * q.z;
-  if (d - cone.w - kConeEps >= q.w) return 2;
-  if (d + cone.w + kConeEps < q.w) return 0;
+// Tile-vs-occulter classification, in FP32 (it only has to be conservative:
+// the exact FP64 predicate decides every pixel it leaves open).
+//   cone  float4 (cx, cy, cz, w): unit centre c rounded to FP32, and w >= the
+//         largest |s - c| over the tile's pixels s, plus kConeMargin32
+//   row   float4 (qx, qy, qz, thr) / |q|: the occulter row scaled to a unit
+//         direction (the same half-space), rounded to FP32
+// Returns 2 if every pixel of the tile is visible, 0 if none is, 1 if the tile
+// must be tested pixel by pixel.  For a unit q, |s.q - c.q| <= |s - c|;
+// kConeMargin32 covers the FP32 roundings (dot product ~2e-7, row and
+// threshold rounding ~2e-7, the +-w below ~2e-7) with a wide safety factor.
+// NaN rows or cones compare false both ways: "test every pixel".
+constexpr double kConeMargin32 = 4e-6;
+__device__ __forceinline__ int cone_state32(const float4 &cone, const float4 &q) {
+  const float d = fmaf(cone.z, q.z, fmaf(cone.y, q.y, cone.x * q.x));
+  if (d - cone.w >= q.w) return 2;
+  if (d + cone.w < q.w) return 0;
   return 1;
 }
 
