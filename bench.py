@@ -48,6 +48,11 @@ WORKLOAD_TEXT = {
 METRIC = "G uvw x pixel terms/s (vis-gen + adjoint), split precision, rel-L2<=1e-5 vs FP64"
 UNIT = "Gterms/s"
 MUFU_TERMS_PER_CLK_PER_SM = 8     # 16 MUFU results/clk/SM, sin + cos per term
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# tuned shapes, from the one-pass ncu capture of this bench command recorded in
+# profiles/dram_c3_10mhz.md; bench.py cannot read DRAM counters itself.
+NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 57271808 + 45663744, "k_adjoint": 61557504 + 45525504}}
+NCU_TRAFFIC_SOURCE = "profiles/dram_c3_10mhz.md (ncu, one pass, full-size workload)"
 
 
 def peaks():
@@ -304,7 +309,9 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": f"8 terms/clk/SM x {nsm} SMs x sm_max_mhz ({pk_kind})",
                      "evaluated_frac": round(dom_eval / (K * J), 4),
                      "frac_of_evaluated": round(dom_eval / dom_s / peak_terms, 4),
-                     "traffic": None},
+                     "traffic": NCU_TRAFFIC.get(args.workload, {}).get(f"k_{dom}"),
+                     "traffic_unit": "bytes per launch",
+                     "traffic_source": NCU_TRAFFIC_SOURCE if args.workload in NCU_TRAFFIC else None},
         "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
         "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_mixed": round(mx_f / tot, 4),
                     "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_mixed": round(mx_a / tot, 4)},

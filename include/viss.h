@@ -100,7 +100,8 @@ double viss_cone_threshold(float R, float h);
 
 /* Mask bits for testing: bit j of row k set iff (sample k, pixel j) is
  * visible under refs (K x 3 int32 rows into occ; -1 = unused).  bits is
- * K x ceil(J/32) uint32. */
+ * K x ceil(J/32) uint32.  Every ref must index a row of occ (the table size
+ * is not passed, so this entry point cannot check it). */
 int viss_mask_bits(int64_t K, int64_t J, const double *lmn, const int32_t *refs,
                    const double *occ, uint32_t *bits, void *stream);
 
@@ -115,7 +116,10 @@ int viss_plan_destroy(viss_plan *plan);
 int viss_plan_set_pixels(viss_plan *plan, int64_t J, const double *lmn, void *stream);
 
 /* Samples: uvw (K x 3 FP64 in wavelengths), off (K FP64 turns, or NULL),
- * refs (K x 3 int32 into occ, or NULL = never occulted), occ (G x 4 FP64). */
+ * refs (K x 3 int32 into occ, or NULL = never occulted), occ (G x 4 FP64).
+ * Refs outside [-1, G) return VISS_ERR_ARG, as do non-finite uvw or off
+ * (VISS_ERR_NOTFINITE); the plan then holds no samples until the next
+ * successful call.  Synchronises `stream` once. */
 int viss_plan_set_samples(viss_plan *plan, int64_t K, const double *uvw, const double *off,
                           const int32_t *refs, int64_t G, const double *occ, void *stream);
 

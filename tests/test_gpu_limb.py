@@ -80,3 +80,23 @@ def test_grazing_rows_adjoint(case, oracle, cuda_device):
         assert np.abs(Cs - Co).max() < 1e-2, (shape, np.abs(Cs - Co).max())
     Cd = plan.adjoint(a_d, fp64=True).cpu().numpy().astype(np.float64)
     assert np.abs(Cd - Co).max() < 1e-3
+
+
+def test_refs_outside_the_table_are_rejected(viss, cuda_device):
+    """A ref past the occulter table (or below -1) is an argument error, not an
+    out-of-bounds read; the plan holds no samples afterwards."""
+    from viss_optimize_3d_b200._capi import VissError
+    lmn = api.pix2lmn(4, "ring", device=cuda_device)
+    uvw = torch.zeros((8, 3), dtype=torch.float64, device=cuda_device)
+    occ = torch.tensor([[0.0, 0.0, 1.0, 0.5]] * 3, dtype=torch.float64, device=cuda_device)
+    for bad in (3, -2):
+        refs = torch.full((8, 3), -1, dtype=torch.int32, device=cuda_device)
+        refs[5, 1] = bad
+        plan = api.Plan(lmn)
+        with pytest.raises(VissError, match="outside"):
+            plan.set_samples(uvw, None, refs, occ)
+        with pytest.raises(VissError):
+            plan.forward(torch.ones(lmn.shape[0], device=cuda_device))
+    refs = torch.full((8, 3), 2, dtype=torch.int32, device=cuda_device)
+    plan = api.Plan(lmn, uvw, None, refs, occ)     # the last row is in range
+    assert plan.forward(torch.ones(lmn.shape[0], device=cuda_device)).shape == (8,)

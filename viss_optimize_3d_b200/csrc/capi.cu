@@ -36,7 +36,8 @@ cudaError_t launch_stage_sky(long long, long long, const double4 *, const int *,
                              float, double4 *, int, cudaStream_t);
 cudaError_t launch_stage_coef(long long, long long, const float2 *, float2 *, cudaStream_t);
 cudaError_t launch_stage_samples(long long, const double *, const double *, const int32_t *,
-                                 double4 *, int4 *, unsigned long long *, cudaStream_t);
+                                 long long, double4 *, int4 *, unsigned long long *, int *,
+                                 cudaStream_t);
 cudaError_t launch_dcf(long long, const float *, int, int, int32_t *, unsigned int *, float *,
                        int, cudaStream_t);
 cudaError_t launch_weights(long long, const float *, const float *, const int32_t *,
@@ -364,17 +365,22 @@ int viss_plan_set_samples(viss_plan *p, int64_t K, const double *uvw, const doub
               "viss_plan_set_samples: occulters");
     VISS_CUDA(viss::launch_occ32(G, p->occ, p->occ32, st), "viss_plan_set_samples: occulters");
   }
-  VISS_CUDA(cudaMemsetAsync(p->dev_words + 3, 0, sizeof(unsigned long long), st),
+  // words [1] (bad-ref flag here; error flags during a kernel) and [3] (phase bound)
+  VISS_CUDA(cudaMemsetAsync(p->dev_words + 1, 0, 3 * sizeof(unsigned long long), st),
             "viss_plan_set_samples");
-  VISS_CUDA(viss::launch_stage_samples(K, uvw, off, refs, p->samp, refs ? p->refs : nullptr,
-                                       p->dev_words + 3, st),
+  p->K = 0;  // not usable until staged and checked
+  VISS_CUDA(viss::launch_stage_samples(K, uvw, off, refs, refs ? G : 0, p->samp,
+                                       refs ? p->refs : nullptr, p->dev_words + 3,
+                                       reinterpret_cast<int *>(p->dev_words + 1), st),
             "viss_plan_set_samples");
-  unsigned long long bits = 0;
-  VISS_CUDA(cudaMemcpyAsync(&bits, p->dev_words + 3, sizeof(bits), cudaMemcpyDeviceToHost, st),
+  unsigned long long words[3] = {0, 0, 0};
+  VISS_CUDA(cudaMemcpyAsync(words, p->dev_words + 1, sizeof(words), cudaMemcpyDeviceToHost, st),
             "viss_plan_set_samples: bound");
   VISS_CUDA(cudaStreamSynchronize(st), "viss_plan_set_samples: sync");
+  if (static_cast<int>(words[0] & 0xffffffffu) != 0)
+    return fail(VISS_ERR_ARG, "viss_plan_set_samples: occulter refs outside [-1, G)");
   double bound;
-  std::memcpy(&bound, &bits, sizeof(bound));
+  std::memcpy(&bound, &words[2], sizeof(bound));
   if (!std::isfinite(bound))
     return fail(VISS_ERR_NOTFINITE, "viss_plan_set_samples: non-finite uvw or offset");
   p->K = K;

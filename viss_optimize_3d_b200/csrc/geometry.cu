@@ -221,14 +221,28 @@ __global__ void k_stage_sky(long long J, long long Jpad, const double4 *pix, con
 }
 
 // Sample staging: uvw (K x 3), off (K or null), refs (K x 3 or null).
+// Sample staging.  Occulter refs outside [-1, G) set *badref and are staged
+// as -1, so the kernels never index past the occulter table.
+__device__ __forceinline__ int checked_ref(int r, long long G, int *badref) {
+  if (r < -1 || r >= G) {
+    atomicOr(badref, 1);
+    return -1;
+  }
+  return r;
+}
+
 __global__ void k_stage_samples(long long K, const double *uvw, const double *off,
-                                const int32_t *refs, double4 *samp, int4 *ref4) {
+                                const int32_t *refs, long long G, double4 *samp, int4 *ref4,
+                                int *badref) {
   const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k >= K) return;
   samp[k] = make_double4(uvw[3 * k], uvw[3 * k + 1], uvw[3 * k + 2], off ? off[k] : 0.0);
   if (ref4) {
-    if (refs) ref4[k] = make_int4(refs[3 * k], refs[3 * k + 1], refs[3 * k + 2], -1);
-    else ref4[k] = make_int4(-1, -1, -1, -1);
+    if (refs)
+      ref4[k] = make_int4(checked_ref(refs[3 * k], G, badref), checked_ref(refs[3 * k + 1], G, badref),
+                          checked_ref(refs[3 * k + 2], G, badref), -1);
+    else
+      ref4[k] = make_int4(-1, -1, -1, -1);
   }
 }
 
@@ -314,10 +328,10 @@ cudaError_t launch_stage_coef(long long K, long long Kpad, const float2 *coef, f
 }
 
 cudaError_t launch_stage_samples(long long K, const double *uvw, const double *off,
-                                 const int32_t *refs, double4 *samp, int4 *ref4,
-                                 unsigned long long *bound, cudaStream_t st) {
+                                 const int32_t *refs, long long G, double4 *samp, int4 *ref4,
+                                 unsigned long long *bound, int *badref, cudaStream_t st) {
   if (K <= 0) return cudaSuccess;
-  k_stage_samples<<<nblk(K, 256), 256, 0, st>>>(K, uvw, off, refs, samp, ref4);
+  k_stage_samples<<<nblk(K, 256), 256, 0, st>>>(K, uvw, off, refs, G, samp, ref4, badref);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !bound) return e;
   k_sample_bound<<<nblk(K, 256), 256, 0, st>>>(K, samp, bound);

@@ -37,7 +37,8 @@
 
 namespace viss {
 cudaError_t launch_stage_samples(long long, const double *, const double *, const int32_t *,
-                                 double4 *, int4 *, unsigned long long *, cudaStream_t);
+                                 long long, double4 *, int4 *, unsigned long long *, int *,
+                                 cudaStream_t);
 cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, float4 *cones,
                               cudaStream_t st);
 cudaError_t launch_occ32(long long G, const double4 *occ, float4 *out, cudaStream_t st);
@@ -160,17 +161,21 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   if ((e = viss::launch_tile_cones(ntiles, pix, cones, st)) != cudaSuccess) return na_cuda(e, "cones");
   if (refs && (e = viss::launch_occ32(G, reinterpret_cast<const double4 *>(occ), occ32, st)) != cudaSuccess)
     return na_cuda(e, "occulters");
-  if ((e = viss::launch_stage_samples(K, uvw, off, refs, samp, refs ? ref4 : nullptr, words + 3,
-                                      st)) != cudaSuccess)
+  if ((e = viss::launch_stage_samples(K, uvw, off, refs, refs ? G : 0, samp,
+                                      refs ? ref4 : nullptr, words + 3,
+                                      reinterpret_cast<int *>(words + 1), st)) != cudaSuccess)
     return na_cuda(e, "stage samples");
 
-  // the split-precision phase needs |u.s + off| < 2^28 turns
-  unsigned long long bits = 0;
-  if ((e = cudaMemcpyAsync(&bits, words + 3, sizeof(bits), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+  // bad-ref flag (word 1) and the |u.s + off| bound (word 3): the split-precision
+  // phase needs |u.s + off| < 2^28 turns
+  unsigned long long w13[3] = {0, 0, 0};
+  if ((e = cudaMemcpyAsync(w13, words + 1, sizeof(w13), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return na_cuda(e, "bound");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return na_cuda(e, "sync");
+  if (static_cast<int>(w13[0] & 0xffffffffu) != 0)
+    return viss::record_error(VISS_ERR_ARG, "viss_forward_noalloc: occulter refs outside [-1, G)");
   double bound;
-  std::memcpy(&bound, &bits, sizeof(bound));
+  std::memcpy(&bound, &w13[2], sizeof(bound));
   if (!std::isfinite(bound))
     return viss::record_error(VISS_ERR_NOTFINITE, "viss_forward_noalloc: non-finite uvw or offset");
   if (!(bound < viss::kMaxTurns))
