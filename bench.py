@@ -44,6 +44,10 @@ WORKLOAD_TEXT = {
           "(45 baselines x 2,880 snapshots), Moon + Earth occultation, spectral index per pixel",
     "c5": "reconstruction: Nside 128 (196,608 px) x 194,400 uvw samples (45 baselines x 4,320 "
           "snapshots), 10 MHz, Moon occultation, SNR 20, positions perturbed N(0, 5 m); 200 L-BFGS steps",
+    "c1": "Nside 32 (12,288 px) x 10,080 uvw samples (28 baselines x 360 snapshots), 1 MHz, "
+          "no occultation",
+    "stream": "day files end to end: Nside 256 (786,432 px) x 388,800 uvw samples + 388,800 mirror "
+              "rows per day, 10 MHz, Moon occultation in both passes; text drop-in vs binary streaming loop",
 }
 METRIC = "G uvw x pixel terms/s (vis-gen + adjoint), split precision, rel-L2<=1e-5 vs FP64"
 UNIT = "Gterms/s"
@@ -211,22 +215,25 @@ def run_ours(args, rank, world, local_rank):
     # end to end through the public API from pinned host buffers
     sky_h = torch.from_numpy(obs.sky_at(f_hz).astype(np.float32) * np.float32(4 * math.pi / J)).pin_memory()
     uvw_h = torch.from_numpy(obs.uvw(f_hz)).pin_memory()
-    refs_h = torch.from_numpy(obs.refs).pin_memory()
+    masked = obs.refs is not None
+    refs_h = torch.from_numpy(obs.refs).pin_memory() if masked else None
     img_h = torch.empty(J, dtype=torch.float32).pin_memory()
     V_h = torch.empty(K, dtype=torch.complex64).pin_memory()
     sky_d = torch.empty_like(g.sky)
     uvw_d = torch.empty_like(g.uvw)
-    refs_d = torch.empty_like(g.refs)
+    refs_d = torch.empty_like(g.refs) if masked else None
     from viss_optimize_3d_b200._capi import check, lib
     import ctypes as C
 
     def e2e_step():
         sky_d.copy_(sky_h, non_blocking=True)
         uvw_d.copy_(uvw_h, non_blocking=True)
-        refs_d.copy_(refs_h, non_blocking=True)
+        if masked:
+            refs_d.copy_(refs_h, non_blocking=True)
         check(lib.viss_plan_set_samples(g.plan._h, K, C.c_void_p(uvw_d.data_ptr()), None,
-                                        C.c_void_p(refs_d.data_ptr()), g.occ.shape[0],
-                                        C.c_void_p(g.occ.data_ptr()),
+                                        C.c_void_p(refs_d.data_ptr()) if masked else None,
+                                        g.occ.shape[0] if masked else 0,
+                                        C.c_void_p(g.occ.data_ptr()) if masked else None,
                                         C.c_void_p(stream.cuda_stream)), "set_samples")
         Vd = g.plan.forward(sky_d)
         imgd = pipeline.dirty_image(g, Vd)
@@ -245,7 +252,7 @@ def run_ours(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_s = e0.elapsed_time(e1) / 1e3
-    h2d = J * 4 + K * 24 + K * 12
+    h2d = J * 4 + K * 24 + (K * 12 if masked else 0)
     d2h = J * 4 + K * 8
 
     # max over ranks (device-timed seconds)
@@ -492,14 +499,16 @@ def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
     lmn = O.lmn_from_xyz(xyz)
     uvw = obs.uvw(f_hz)
     sky = obs.sky_at(f_hz) * (4 * math.pi / obs.cfg.npix)
-    occ = O.occulters(obs.occ_sat_positions, 1737.4e3, 0)
-    if obs.earth_rows is not None:
-        occ = np.concatenate([occ, obs.earth_rows])
-    refs = obs.refs
+    refs, occ = obs.refs, None
+    if refs is not None:
+        occ = O.occulters(obs.occ_sat_positions, 1737.4e3, 0)
+        if obs.earth_rows is not None:
+            occ = np.concatenate([occ, obs.earth_rows])
+    sel = (lambda r, idx: None if r is None else r[idx])
     K, J = uvw.shape[0], lmn.shape[0]
     # calibrate on a tiny slice
     t0 = time.perf_counter()
-    O.forward(uvw[:cores], lmn, sky, refs[:cores], occ, nthreads=cores)
+    O.forward(uvw[:cores], lmn, sky, sel(refs, slice(0, cores)), occ, nthreads=cores)
     rate = cores * J / max(time.perf_counter() - t0, 1e-6)       # terms/s
     n_f = int(max(cores, min(K, 0.5 * budget_s * rate / J)))
     n_a = int(max(cores, min(J, 0.5 * budget_s * rate / K)))
@@ -508,7 +517,7 @@ def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
     js = np.sort(rng.choice(J, n_a, replace=False))
     a = np.ones(K, dtype=np.complex128)
     t0 = time.perf_counter()
-    O.forward(uvw[ks], lmn, sky, refs[ks], occ, nthreads=cores)
+    O.forward(uvw[ks], lmn, sky, sel(refs, ks), occ, nthreads=cores)
     t1 = time.perf_counter()
     O.adjoint(uvw, a, lmn[js], refs, occ, nthreads=cores)
     t2 = time.perf_counter()
@@ -521,6 +530,94 @@ def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
 
 
 # ---------------------------------------------------------- reference arm
+def run_stream(args):
+    """Observation days from files to images, wall clock, three ways on the same
+    synthetic days: the text drop-in executable (the reference's interface and
+    file formats, one day after another), the binary streaming loop, and the
+    loop with --fold-mirrors.  Terms per day are counted in the headline unit
+    (forward + adjoint over the unique samples)."""
+    import dataclasses
+    import shutil
+    import subprocess
+    import tempfile
+
+    import numpy as np
+    from viss_optimize_3d_b200 import api, dayfile, synth
+
+    cfg = synth.CONFIGS["c3_10mhz"]
+    f_hz, ndays = 1e7, args.stream_days
+    bindir = os.path.join(ROOT, "viss_optimize_3d_b200", "bin")
+    work = tempfile.mkdtemp(prefix="viss_stream_")
+    try:
+        th, ph, _ = api.pix2ang(cfg.nside, "ring")
+        th, ph = th.cpu().numpy().astype(np.float32), ph.cpu().numpy().astype(np.float32)
+        sky = synth.make_observation(cfg).sky.astype(np.float32)
+        tdir, bdir = os.path.join(work, "earth_10Mhz"), os.path.join(work, "bin")
+        for d in (tdir, bdir, os.path.join(work, "out_text")):
+            os.makedirs(d)
+        dayfile.write_sky(os.path.join(bdir, "sky.vsky"), sky, th, ph)
+        with open(os.path.join(tdir, "B_10Mhz.txt"), "w") as fh:
+            fh.write(f"{sky.size}\n")
+            np.savetxt(fh, sky, fmt="%.9g")
+        np.savetxt(os.path.join(tdir, "theta_heal_10Mhz.txt"), th, fmt="%.9g")
+        np.savetxt(os.path.join(tdir, "phi_heal_10Mhz.txt"), ph, fmt="%.9g")
+        n_unique = 0
+        for d in range(1, ndays + 1):
+            rows = dayfile.observation_rows(
+                synth.make_observation(dataclasses.replace(cfg, day=float(d - 1))), f_hz)
+            n_unique = rows.uvw.shape[0] // 2
+            dayfile.write_day(dayfile.day_path(bdir, d), rows, day=d, frequency=f_hz)
+            for name, arr in (("uvw", rows.uvw), ("xyza", rows.xyza), ("xyzb", rows.xyzb)):
+                with open(os.path.join(tdir, f"{name}{d}day1M.txt"), "w") as fh:
+                    fh.write("0 0 0\n")
+                    np.savetxt(fh, arr, fmt="%.9g")
+            with open(os.path.join(tdir, f"bll{d}day1M.txt"), "w") as fh:
+                fh.write("0\n")
+                np.savetxt(fh, rows.bll, fmt="%.9g")
+
+        def timed(cmd):
+            t0 = time.perf_counter()
+            r = subprocess.run(cmd, cwd=work, capture_output=True, text=True, timeout=3600)
+            dt = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError(f"{cmd[0]} failed: {r.stderr[-2000:]}")
+            return dt, r.stdout
+
+        t_text, _ = timed([os.path.join(bindir, "vissgen3d_blockage_10m"), "--days", str(ndays),
+                           "--data-dir", tdir, "--out-dir", os.path.join(work, "out_text")])
+        base = [os.path.join(bindir, "vissgen_stream"), "--sky", os.path.join(bdir, "sky.vsky"),
+                "--days-dir", bdir, "--days", str(ndays), "--frequency", str(f_hz), "--blockage", "1"]
+        t_bin, out_bin = timed(base + ["--sum-out", os.path.join(work, "sum.vimg")])
+        t_fold, out_fold = timed(base + ["--fold-mirrors", "--sum-out", os.path.join(work, "sum_fold.vimg")])
+        # the same work: day sums of the three runs agree
+        text_sum = sum(np.loadtxt(os.path.join(work, "out_text", f"C{d}day1M.txt"))
+                       for d in range(1, ndays + 1))
+        s_bin = dayfile.read_image(os.path.join(work, "sum.vimg"))[0]
+        s_fold = dayfile.read_image(os.path.join(work, "sum_fold.vimg"))[0]
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        terms_day = 2 * n_unique * cfg.npix
+        info_bin = json.loads(out_bin.strip().splitlines()[-1])
+        info_fold = json.loads(out_fold.strip().splitlines()[-1])
+
+        def line(t):
+            return {"days_per_s": round(ndays / t, 4), "s_per_day": round(t / ndays, 4),
+                    "gterms_per_s_e2e": round(terms_day * ndays / t / 1e9, 2)}
+        return {"metric": "observation days/s, files to images (wall clock)", "unit": "days/s",
+                "value": round(ndays / t_fold, 4), "higher_is_better": True, "n_gpus": 1,
+                "days": ndays, "data": "synthetic (seeded lunar-orbit formation, see synth.py)",
+                "config": {"workload": WORKLOAD_TEXT["stream"], "pixels": cfg.npix,
+                           "unique_samples_per_day": n_unique, "terms_per_day": terms_day},
+                "text_drop_in": line(t_text), "binary_stream": line(t_bin),
+                "binary_stream_fold_mirrors": line(t_fold),
+                "stream_gpu_ms_per_day": round(info_bin["gpu_ms_total"] / ndays, 2),
+                "stream_fold_gpu_ms_per_day": round(info_fold["gpu_ms_total"] / ndays, 2),
+                "day_sum_rel_l2": {"binary_vs_text": rel(s_bin, text_sum),
+                                   "fold_vs_binary": rel(s_fold, s_bin)},
+                "speedup_vs_text": round(t_text / t_fold, 2)}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -565,6 +662,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOAD_TEXT),
                     help="benchmark configuration (default: the headline one)")
+    ap.add_argument("--stream-days", type=int, default=4,
+                    help="days of the stream workload")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -589,6 +688,9 @@ def main():
             return
         if args.workload == "c5":
             print(json.dumps(run_reconstruction(args)), flush=True)
+            return
+        if args.workload == "stream":
+            print(json.dumps(run_stream(args)), flush=True)
             return
         res = run_ours(args, rank, world, local_rank)
         if res is not None:

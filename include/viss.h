@@ -213,6 +213,24 @@ int viss_wrot(int64_t n, const float *w, float *V, void *stream);
 int viss_conj_mirror(int64_t mirror, float *V, void *stream);
 int viss_scale_coef(int64_t n, const float *wt, const float *V, float *coef, void *stream);
 
+/* ------------------------------------------------------------ day streaming
+ * One observation day's rows (n = unique rows + their mirrors, as in the
+ * reference's per-day files, vissgen3d_blockage.cu:309-391) staged on the
+ * device: replaces the host loops of the reference's vissGen that build the
+ * per-row geometry.  Inputs are FP32 rows (x, y, z) of uvw, xyza, xyzb
+ * (device, n x 3 each); outputs (device): uvw (n x 3 FP64), off (n, = -w, the
+ * forward's w(n-1) term, :95), P (2n x 3 FP64: satellite a of row i at row i,
+ * satellite b at row n + i), refs (n x 3 int32 = (i, n + i, -1)), w (n FP32).
+ * n < 2^30. */
+int viss_stage_day_rows(int64_t n, const float *uvw3, const float *xyza3, const float *xyzb3,
+                        double *uvw, double *off, double *P, int32_t *refs, float *w,
+                        void *stream);
+
+/* sum[j] += img[j] for n pixels in FP64, non-finite pixels counted as 0: the
+ * day sum the reference's notebooks form on the host with NaN -> 0
+ * (healpix3d_blockage.ipynb:103-116), kept on the device. */
+int viss_accumulate_image(int64_t n, const float *img, double *sum, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

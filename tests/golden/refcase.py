@@ -72,8 +72,9 @@ def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10):
     return dict(theta=theta, phi=phi, B=B, uvw=uvw, xyza=xyza, xyzb=xyzb, bll=bll2)
 
 
-def write_inputs(case, root: str, variant_10m: bool = True):
-    """The reference's input files under root (earth_10Mhz/ or earth_1Mhz/)."""
+def write_inputs(case, root: str, variant_10m: bool = True, day: int = 1):
+    """The reference's input files under root (earth_10Mhz/ or earth_1Mhz/),
+    the rows as day `day`."""
     d = os.path.join(root, "earth_10Mhz" if variant_10m else "earth_1Mhz")
     os.makedirs(d, exist_ok=True)
     suffix = "_10Mhz.txt" if variant_10m else ".txt"
@@ -85,10 +86,10 @@ def write_inputs(case, root: str, variant_10m: bool = True):
         with open(os.path.join(d, name + "_heal" + suffix), "w") as f:
             f.writelines(_fmt(x) + "\n" for x in case[name])
     for name in ("uvw", "xyza", "xyzb"):
-        with open(os.path.join(d, name + "1day1M.txt"), "w") as f:
+        with open(os.path.join(d, f"{name}{day}day1M.txt"), "w") as f:
             f.write("0 0 0\n")                                 # first row, skipped
             f.writelines(" ".join(_fmt(v) for v in row) + "\n" for row in case[name])
-    with open(os.path.join(d, "bll1day1M.txt"), "w") as f:
+    with open(os.path.join(d, f"bll{day}day1M.txt"), "w") as f:
         f.write("0\n")                                         # first token, skipped
         f.writelines(_fmt(x) + "\n" for x in case["bll"])
     return d

@@ -23,7 +23,8 @@ BUILD = os.path.join(PKG, "_build_obj")
 LIB = os.path.join(PKG, "libviss.so")
 BIN = os.path.join(PKG, "bin")
 
-CU_SOURCES = ["healpix.cu", "geometry.cu", "visibility.cu", "dcf.cu", "capi.cu", "noalloc.cu"]
+CU_SOURCES = ["healpix.cu", "geometry.cu", "visibility.cu", "dcf.cu", "capi.cu", "noalloc.cu",
+              "days.cu"]
 HEADERS = ["viss_common.cuh", "visibility.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -86,6 +87,8 @@ HOST_PROGRAMS = {
     "vissgen3d_blockage_10m": ("vissgen_main.cpp", ["-DVISS_VARIANT_BLOCKAGE=1", "-DVISS_VARIANT_10M=1"]),
     "vissgen3d_noblockage": ("vissgen_main.cpp", ["-DVISS_VARIANT_BLOCKAGE=0", "-DVISS_VARIANT_10M=0"]),
     "vissgen3d_noblockage_10m": ("vissgen_main.cpp", ["-DVISS_VARIANT_BLOCKAGE=0", "-DVISS_VARIANT_10M=1"]),
+    # streaming day loop over binary day files (not a drop-in: new interface)
+    "vissgen_stream": ("vissgen_stream_main.cpp", []),
 }
 
 

@@ -70,6 +70,8 @@ _SIGS = {
     "viss_wrot": (_i, [_i64, _v, _v, _v]),
     "viss_conj_mirror": (_i, [_i64, _v, _v]),
     "viss_scale_coef": (_i, [_i64, _v, _v, _v, _v]),
+    "viss_stage_day_rows": (_i, [_i64, _v, _v, _v, _v, _v, _v, _v, _v, _v]),
+    "viss_accumulate_image": (_i, [_i64, _v, _v, _v]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
