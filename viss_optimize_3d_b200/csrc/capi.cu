@@ -325,7 +325,8 @@ int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *strea
   const long long nt = Jpad / viss::kTilePix;
   if (int s = ensure(p->pix, p->pix_cap, sizeof(double4) * Jpad, "pixel records")) return s;
   if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * Jpad, "pixel+sky records")) return s;
-  if (int s = ensure(p->cones, p->cones_cap, sizeof(float4) * 5 * nt, "tile cones")) return s;
+  if (int s = ensure(p->cones, p->cones_cap, sizeof(float4) * viss::cone_count(nt), "tile cones"))
+    return s;
   if (int s = ensure(p->perm, p->perm_cap, sizeof(int) * J, "pixel order")) return s;
   const cudaStream_t st = as_stream(stream);
   // compact tiles: order the pixels by a hierarchical (NESTED) locality key

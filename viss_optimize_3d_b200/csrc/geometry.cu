@@ -193,6 +193,34 @@ __global__ void k_tile_cones(long long ntiles, const double4 *pix, float4 *cones
   if (lane == 0) cones[t] = tile;
 }
 
+// Super-tile cones: the cone enclosing the FP32 cones of tiles
+// [kSuperTiles s, kSuperTiles (s + 1)) at cones[5 ntiles + s].  Centre =
+// normalised sum of the tile centres rounded to FP32; radius = the largest
+// chord to a tile centre plus that tile's radius (which already carries
+// kConeMargin32), rounded up: every pixel of every tile lies within it.
+__global__ void k_super_cones(long long ntiles, float4 *cones) {
+  const long long s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long nsup = (ntiles + kSuperTiles - 1) / kSuperTiles;
+  if (s >= nsup) return;
+  const long long t0 = s * kSuperTiles, t1 = min(t0 + kSuperTiles, ntiles);
+  double sx = 0, sy = 0, sz = 0;
+  bool bad = false;
+  for (long long t = t0; t < t1; ++t) {
+    const float4 c = cones[t];
+    sx += c.x; sy += c.y; sz += c.z;
+    bad = bad || isnan(c.w);
+  }
+  bool degenerate;
+  float4 sc = cone_centre(sx, sy, sz, degenerate);
+  double r = 0;
+  for (long long t = t0; t < t1; ++t) {
+    const float4 c = cones[t];
+    r = fmax(r, chord(c.x, c.y, c.z, sc) + static_cast<double>(c.w));
+  }
+  sc.w = bad ? __int_as_float(0x7fc00000) : (degenerate ? 4.f : __double2float_ru(r + 1e-9));
+  cones[5 * ntiles + s] = sc;
+}
+
 // FP32 occulter rows for the classification: (q, thr) / |q| (the same
 // half-space with a unit direction); rows with |q| = 0 or non-finite |q| are
 // rounded as they are (NaN stays NaN: "test every pixel").
@@ -295,6 +323,8 @@ cudaError_t launch_stage_pixels(long long J, long long Jpad, const double *lmn, 
   if (e != cudaSuccess) return e;
   const long long nt = Jpad / kTilePix;
   k_tile_cones<<<nblk(nt, 8), 256, 0, st>>>(nt, pix, cones);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_super_cones<<<nblk((nt + kSuperTiles - 1) / kSuperTiles, 256), 256, 0, st>>>(nt, cones);
   return cudaGetLastError();
 }
 
@@ -359,6 +389,9 @@ cudaError_t sort_pixel_keys(long long J, unsigned long long *keys_in, unsigned l
 cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, float4 *cones, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   k_tile_cones<<<nblk(ntiles, 8), 256, 0, st>>>(ntiles, pix, cones);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_super_cones<<<nblk((ntiles + kSuperTiles - 1) / kSuperTiles, 256), 256, 0, st>>>(ntiles, cones);
   return cudaGetLastError();
 }
 

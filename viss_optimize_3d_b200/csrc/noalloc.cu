@@ -54,8 +54,9 @@ constexpr int kNaMaxChunks = 8;          // cross-block partial sums per sample
 
 // Byte offsets of the regions inside the array (each a multiple of 256).
 constexpr size_t kOffPix = 0;                                        // double4[kNaMaxPix]
-constexpr size_t kOffCones = kOffPix + 32ull * kNaMaxPix;            // float4[5 * kNaMaxPix/128]
-constexpr size_t kOffOcc32 = kOffCones + 16ull * 5 * (kNaMaxPix / viss::kTilePix);  // float4[kNaMaxOcc]
+constexpr size_t kOffCones = kOffPix + 32ull * kNaMaxPix;            // float4[cone_count(kNaMaxPix/128)]
+constexpr size_t kOffOcc32 =
+    kOffCones + (16ull * viss::cone_count(kNaMaxPix / viss::kTilePix) + 255) / 256 * 256;  // float4[kNaMaxOcc]
 constexpr size_t kOffSamp = kOffOcc32 + 16ull * kNaMaxOcc;           // double4[kNaMaxSamp]
 constexpr size_t kOffRefs = kOffSamp + 32ull * kNaMaxSamp;           // int4[kNaMaxSamp]
 constexpr size_t kOffPart = kOffRefs + 16ull * kNaMaxSamp;           // double2[chunks][kNaMaxSamp]

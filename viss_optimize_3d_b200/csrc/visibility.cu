@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   __syncthreads();
 
   unsigned long long evaluated = 0, mixed_terms = 0;
+  unsigned sup = 0;  // per-row super-tile states (MASKED)
   int next = 0;  // next tile to issue (producer state, thread 0)
   for (int it = 0; it < ntile; ++it) {
     const int t = t0 + it, stage = it % S;
@@ -296,12 +297,24 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
 #pragma unroll
     for (int r = 0; r < R; ++r) st[r] = 2;
     if (MASKED) {
+      // once per super-tile: samples wholly visible (2) or wholly hidden (0)
+      // there skip the per-tile test; 1 = test each tile (2 bits per row)
+      if (it == 0 || (t & (kSuperTiles - 1)) == 0) {
+        const float4 sc = p.cones[5LL * p.ntiles + t / kSuperTiles];
+        sup = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int s = kval[r] ? (sample_state(s_refs[r][tid], sc, p.occ32) & 3) : 2;
+          sup |= static_cast<unsigned>(s) << (2 * r);
+        }
+      }
       const float4 cone = p.cones[t];
       bool full = true, any = false;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if (kval[r]) {
-          st[r] = sample_state(s_refs[r][tid], cone, p.occ32);
+          const unsigned known = (sup >> (2 * r)) & 3u;
+          st[r] = known != 1 ? static_cast<int>(known) : sample_state(s_refs[r][tid], cone, p.occ32);
           full = full && (st[r] == 2);
           any = any || ((st[r] & 3) != 0);
         }

@@ -8,7 +8,8 @@
 //   occulter      double4 (qx, qy, qz, thr)  32 B / occulter (exact test)
 //   occulter32    float4 (q, thr) / |q|      16 B / occulter (classification)
 //   cones         float4 (cx, cy, cz, w)     16 B per pixel tile, then 4 x 16 B
-//                 per tile for its 32-pixel sub-tiles (see cone_state32)
+//                 per tile for its 32-pixel sub-tiles, then 16 B per super-tile of
+//                 kSuperTiles tiles (see cone_state32 and cone_count)
 #pragma once
 
 #include <cstdint>
@@ -19,6 +20,17 @@ namespace viss {
 // Pixels per tile: one forward tile staged in shared memory, and one warp's
 // pixel set in the adjoint (32 lanes x 4 pixels).
 constexpr int kTilePix = 128;
+
+// Tiles per super-tile: the forward classifies a sample once per super-tile
+// and skips the per-tile test where the super-tile is wholly visible or
+// wholly hidden for it.
+constexpr int kSuperTiles = 8;
+
+// float4 entries of the cone array for ntiles tiles: tile cones [0, nt),
+// sub-tile cones [nt, 5 nt), super-tile cones [5 nt, 5 nt + ceil(nt / 8)).
+__host__ __device__ constexpr long long cone_count(long long ntiles) {
+  return 5 * ntiles + (ntiles + kSuperTiles - 1) / kSuperTiles;
+}
 
 // Phase-to-fixed-point constant: t = kMagic + u.s + off lands in [2^29, 2^30)
 // for |u.s + off| < 2^28 turns, where one ulp of a double is 2^-23 turn.  The
