@@ -55,7 +55,7 @@ MUFU_TERMS_PER_CLK_PER_SM = 8     # 16 MUFU results/clk/SM, sin + cos per term
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # tuned shapes, from the one-pass ncu capture of this bench command recorded in
 # profiles/dram_c3_10mhz.md; bench.py cannot read DRAM counters itself.
-NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 57271808 + 45663744, "k_adjoint": 61557504 + 45525504}}
+NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 56217088 + 45796096, "k_adjoint": 60853248 + 45885696}}
 NCU_TRAFFIC_SOURCE = "profiles/dram_c3_10mhz.md (ncu, one pass, full-size workload)"
 
 
