@@ -622,7 +622,13 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     from viss_optimize_3d_b200 import synth
-    cfg = synth.CONFIGS[WORKLOAD]
+    if args.workload == "c3_small":
+        cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
+    elif args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz"):
+        cfg = synth.CONFIGS[args.workload]
+    else:
+        return {"impl": "reference", "unavailable": f"workload {args.workload} has no reference "
+                "counterpart (batched channels, reconstruction and day files are this repository's)"}
     obs = synth.make_observation(cfg)
     f_hz = cfg.freqs_hz[0]
     vals = []
@@ -640,7 +646,8 @@ def run_reference(args, rank, world):
         "ms_per_step": round(terms / (v * 1e9) * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (same generator and seed as our arm)",
-        "config": {"workload": "Nside 256 x 388,800 uvw samples, 10 MHz, Moon + Earth",
+        "config": {"workload": WORKLOAD_TEXT.get(args.workload, args.workload),
+                   "pixels": obs.cfg.npix, "samples": obs.cfg.n_samples, "terms_per_step": terms,
                    "note": "the reference has no CPU implementation; this is the FP64 "
                            "restatement of its kernels (oracle/), timed on a bounded sample"},
         "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": last["cores"],
