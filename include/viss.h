@@ -156,6 +156,15 @@ int viss_plan_tune(viss_plan *plan, const float *sky, const float *coef, float *
  * frequency per executable, vissgen3d_blockage.cu:568). */
 int viss_plan_set_channels(viss_plan *plan, int channels);
 
+/* Test hook for the failure path: the next viss_forward or viss_adjoint on
+ * this plan has its first thread block skip the staging copy of its `tile`-th
+ * tile (a pixel tile in the forward, a sample tile in the adjoint), so that
+ * block's bounded waits give up (about 1 s each, no fault, no trap), the
+ * kernel ends, and viss_plan_last_stats / viss_plan_last_counts then return
+ * VISS_ERR_TIMEOUT; the plan and the context stay usable.  The results of
+ * that one call are incomplete.  No counterpart in the reference. */
+int viss_plan_debug_drop_copy(viss_plan *plan, int tile);
+
 /* Sets the launch shapes directly (indices 0..3 each). */
 int viss_plan_set_shapes(viss_plan *plan, int fwd_shape, int adj_shape);
 

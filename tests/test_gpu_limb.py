@@ -100,3 +100,26 @@ def test_refs_outside_the_table_are_rejected(viss, cuda_device):
     refs = torch.full((8, 3), 2, dtype=torch.int32, device=cuda_device)
     plan = api.Plan(lmn, uvw, None, refs, occ)     # the last row is in range
     assert plan.forward(torch.ones(lmn.shape[0], device=cuda_device)).shape == (8,)
+
+
+@pytest.mark.parametrize("which", ["forward", "adjoint"])
+def test_bounded_wait_reports_a_lost_copy(case, cuda_device, which):
+    """Failure path without a GPU fault: the first thread block never receives
+    one staging copy (viss_plan_debug_drop_copy), its bounded waits give up
+    after about a second, the kernel ends and the call reports
+    VISS_ERR_TIMEOUT; the same plan then computes the right result again."""
+    from viss_optimize_3d_b200._capi import VissError, check, lib
+    lmn, uvw, sky, refs, occ, plan = case
+    plan.set_shapes(0, 0)
+    sky_d = torch.as_tensor(sky, dtype=torch.float32, device=cuda_device)
+    a = torch.ones(len(uvw), dtype=torch.complex64, device=cuda_device)
+    run = (lambda: plan.forward(sky_d)) if which == "forward" else (lambda: plan.adjoint(a))
+    good = run().cpu()
+    plan.last_stats()
+    check(lib.viss_plan_debug_drop_copy(plan._h, 1), "viss_plan_debug_drop_copy")
+    run()
+    with pytest.raises(VissError, match="bounded device wait"):
+        plan.last_stats()
+    again = run().cpu()
+    plan.last_stats()                                  # no error: the flag was per call
+    assert torch.equal(again, good)

@@ -138,6 +138,7 @@ struct viss_plan {
   // launch shape
   int fwd_shape = 0;   // index into viss::kFwdShapes (viss_plan_tune picks it)
   int adj_shape = 0;   // index into viss::kAdjShapes
+  int drop_tile = -1;  // test hook for the next kernel (viss_plan_debug_drop_copy)
   int fwd_waves = 16;
   int adj_waves = 16;
 };
@@ -429,6 +430,8 @@ static int forward_impl(viss_plan *p, const float *sky, float *V, int flags, cud
   fp.channels = p->channels;
   fp.Kc = p->Kc;
   fp.pix_stride = p->Jpad;
+  fp.drop_tile = p->drop_tile;
+  p->drop_tile = -1;
   VISS_CUDA(viss::launch_forward(fp, shape, real_chunks, masked, fp64, st), "viss_forward: kernel");
   VISS_CUDA(viss::launch_reduce_fwd(p->K, real_chunks, fp.part, reinterpret_cast<float2 *>(V),
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
@@ -481,6 +484,8 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
   ap.channels = p->channels;
   ap.Kc = p->Kc;
   ap.nchunk = nchunk;
+  ap.drop_tile = p->drop_tile;
+  p->drop_tile = -1;
   VISS_CUDA(viss::launch_adjoint(ap, shape, nchunk, masked, fp64, st), "viss_adjoint: kernel");
   VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, p->channels, ap.part, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
@@ -552,6 +557,12 @@ int viss_plan_set_channels(viss_plan *p, int channels) {
   if (channels > 65535) return fail(VISS_ERR_ARG, "viss_plan_set_channels: at most 65535 channels");
   p->channels = channels;
   p->Kc = Kc;
+  return VISS_OK;
+}
+
+int viss_plan_debug_drop_copy(viss_plan *p, int tile) {
+  if (!p || tile < 0) return fail(VISS_ERR_ARG, "viss_plan_debug_drop_copy: bad arguments");
+  p->drop_tile = tile;
   return VISS_OK;
 }
 

@@ -212,6 +212,7 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   fp.channels = 1;
   fp.Kc = K;
   fp.pix_stride = Jpad;
+  fp.drop_tile = -1;
   if ((e = viss::launch_forward(fp, shape, real_chunks, refs != nullptr, false, st)) != cudaSuccess)
     return na_cuda(e, "forward kernel");
   if ((e = viss::launch_reduce_fwd(K, real_chunks, part, reinterpret_cast<float2 *>(V), 0, st)) !=

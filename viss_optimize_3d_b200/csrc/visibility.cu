@@ -264,7 +264,11 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
   const int t0 = blockIdx.y * p.tiles_per_chunk;
   const int ntile = max(0, min(t0 + p.tiles_per_chunk, p.ntiles) - t0);
   constexpr uint32_t kTileBytes = kTilePix * sizeof(double4);
+  // test hook (viss_plan_debug_drop_copy): the first CTA never stages one
+  // tile, so its bounded waits run out and the error flag is raised
+  const int drop = (blockIdx.x == 0 && blockIdx.y == 0) ? p.drop_tile : -1;
   auto issue = [&](int i, int stage) {
+    if (i == drop) return;
     mbar_expect_tx(&s_full[stage], kTileBytes);
     bulk_g2s(s_pix[stage], pix + static_cast<long long>(t0 + i) * kTilePix, kTileBytes,
              &s_full[stage]);
@@ -537,7 +541,10 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   const long long k1 = min(k0 + p.samples_per_chunk, (ch + 1) * p.Kc);
   const int ntile = static_cast<int>((k1 - k0 + kSampTile - 1) / kSampTile);
 
+  // test hook (viss_plan_debug_drop_copy), as in the forward
+  const int drop = (blockIdx.x == 0 && blockIdx.y == 0) ? p.drop_tile : -1;
   auto issue = [&](int i, int stage) {
+    if (i == drop) return;
     const long long kk = k0 + static_cast<long long>(i) * kSampTile;
     const int n = static_cast<int>(min(static_cast<long long>(kSampTile), k1 - kk));
     // sizes in multiples of 16 B: samp 32 B each, coef 8 B each (pad to even), refs 16 B

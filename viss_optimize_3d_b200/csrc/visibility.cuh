@@ -27,6 +27,7 @@ struct FwdParams {
   int channels;                 // channel-major sample axis: K = channels * Kc
   long long Kc;                 // samples per channel
   long long pix_stride;         // pixel records per channel's sky (Jpad)
+  int drop_tile;                // test hook: CTA (0, 0) skips this tile's copy (-1: none)
 };
 
 struct AdjParams {
@@ -47,6 +48,7 @@ struct AdjParams {
   int channels;                 // one image per channel; K = channels * Kc
   long long Kc;                 // samples per channel (even when channels > 1)
   int nchunk;                   // sample chunks per channel (gridDim.y = channels * nchunk)
+  int drop_tile;                // test hook: CTA (0, 0) skips this tile's copy (-1: none)
 };
 
 struct FwdShape { int R, minb; };
