@@ -10,7 +10,9 @@
   images, --fold-mirrors and --fp64 within 1e-5 (rel-L2) of it;
 * errors: a truncated day file, a missing day, non-mirrored rows under
   --fold-mirrors, each a non-zero exit with a message (no GPU fault involved:
-  all are found on the host).
+  all are found on the host);
+* --resume: finished days are taken from their image files, a missing one is
+  recomputed bit-identically, the day sum agrees.
 """
 import dataclasses
 import json
@@ -153,3 +155,31 @@ def test_errors_are_reported(three_days, tmp_path):
     dayfile.write_day(bad / "day1.vday", rows, day=1)
     r = run("vissgen_stream", *base, "--days", "1", "--fold-mirrors", ok=False)
     assert r.returncode != 0 and "exact mirrors" in r.stderr
+
+
+def test_resume_skips_finished_days(three_days, tmp_path):
+    """--resume: days whose image an earlier run wrote are not recomputed but
+    added to the day sum from their files; a missing day image is recomputed,
+    bit-identical to the first run's."""
+    root, cfg, _ = three_days
+    total = dayfile.read_image(root / "sum.vimg")[0]
+    out = tmp_path / "out"
+    shutil.copytree(root / "out", out)
+    base = ["--sky", root / "bin" / "sky.vsky", "--days-dir", root / "bin", "--days", "3",
+            "--frequency", "1e6", "--blockage", "1", "--out-dir", out, "--resume"]
+    r = run("vissgen_stream", *base, "--sum-out", tmp_path / "s1.vimg")
+    info = json.loads(r.stdout.strip().splitlines()[-1])
+    assert info["resumed_days"] == 3 and info["per_day"] == []
+    s1 = dayfile.read_image(tmp_path / "s1.vimg")[0]
+    np.testing.assert_allclose(s1, total, rtol=1e-12, atol=1e-12 * np.abs(total).max())
+    os.remove(out / "C2.vimg")
+    r = run("vissgen_stream", *base, "--sum-out", tmp_path / "s2.vimg")
+    info = json.loads(r.stdout.strip().splitlines()[-1])
+    assert info["resumed_days"] == 2 and [d[0] for d in info["per_day"]] == [2]
+    s2 = dayfile.read_image(tmp_path / "s2.vimg")[0]
+    np.testing.assert_allclose(s2, total, rtol=1e-12, atol=1e-12 * np.abs(total).max())
+    again = dayfile.read_image(out / "C2.vimg")[0]
+    assert np.array_equal(again, dayfile.read_image(root / "out" / "C2.vimg")[0])
+    r = run("vissgen_stream", "--sky", root / "bin" / "sky.vsky", "--days-dir", root / "bin",
+            "--resume", ok=False)
+    assert r.returncode != 0 and "--resume needs --out-dir" in r.stderr

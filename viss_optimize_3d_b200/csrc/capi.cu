@@ -4,6 +4,7 @@
 // and calls exit(1).  Every entry point here returns a status instead and
 // records the message in a thread-local string (viss_last_error).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -450,7 +451,14 @@ static int check_call(viss_plan *p, const void *in, const void *out, int flags, 
   return VISS_OK;
 }
 
+// One NVTX range per forward / adjoint call (host side; visible to profilers).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
 int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stream) {
+  const NvtxRange range("viss_forward");
   if (int s = check_call(p, sky, V, flags, "viss_forward")) return s;
   return forward_impl(p, sky, V, flags, as_stream(stream), p->fwd_shape);
 }
@@ -496,6 +504,7 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
 }
 
 int viss_adjoint(viss_plan *p, const float *coef, float *image, float scale, int flags, void *stream) {
+  const NvtxRange range("viss_adjoint");
   if (int s = check_call(p, coef, image, flags, "viss_adjoint")) return s;
   return adjoint_impl(p, coef, image, scale, flags, as_stream(stream), p->adj_shape);
 }

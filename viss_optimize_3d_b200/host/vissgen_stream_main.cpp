@@ -26,7 +26,11 @@
 //
 //   vissgen_stream --sky SKY.vsky --days-dir DIR [--first-day D] [--days N]
 //                  [--frequency HZ] [--blockage 0|1] [--fold-mirrors] [--fp64]
-//                  [--out-dir DIR] [--sum-out FILE] [--devices N]
+//                  [--out-dir DIR [--resume]] [--sum-out FILE] [--devices N]
+// --resume skips the days whose image an earlier run already wrote to
+// --out-dir (a valid C{d}.vimg) and adds those images to the day sum instead,
+// so an interrupted run continues where it stopped.  Each day is one NVTX
+// range ("day d") for profilers.
 //   vissgen_stream --convert-text SRC --to DST [--text-10m] [--first-day D] [--days N]
 //   vissgen_stream --info FILE
 // Prints one JSON line with the timings at the end of a run.
@@ -45,6 +49,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "dayfile.h"
 #include "textio.h"
 #include "viss.h"
@@ -57,7 +63,7 @@ struct Options {
   std::string sky, days_dir, out_dir, sum_out;
   int first_day = 1, days = 1, max_devices = 1 << 20;
   double frequency = 1e6;
-  bool blockage = true, fold = false, fp64 = false;
+  bool blockage = true, fold = false, fp64 = false, resume = false;
   std::string convert_src, convert_dst, info;
   bool text_10m = false;
 };
@@ -192,6 +198,7 @@ class DevicePipeline {
       // the slot's fields belong to the loader again once `loaded` is cleared
       const int64_t n = s.n;
       const int day = s.day;
+      nvtxRangePushA(("day " + std::to_string(day)).c_str());
       cucall(cudaEventRecord(e0, cs_), "event");
       ensure_rows(n);
       cucall(cudaStreamWaitEvent(cs_, s.copied, 0), "wait");
@@ -216,6 +223,7 @@ class DevicePipeline {
       cucall(cudaEventSynchronize(e1), "sync");
       float ms = 0;
       cucall(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+      nvtxRangePop();
       timings.push_back({day, n, ms});
     }
     loader.join();
@@ -455,22 +463,50 @@ class DevicePipeline {
   DevBuf<uint32_t> counts_;
 };
 
+// A day image written by an earlier run, if `path` holds a valid one.
+bool read_day_image(const std::string &path, int64_t npix, std::vector<float> &img) {
+  FileHeader h;
+  std::string err;
+  std::FILE *f = viss_host::open_checked(path, "VISSIMG", 1, h, err);
+  if (!f) return false;
+  bool ok = h.elem_bytes == 4 && h.count == npix && h.days == 1;
+  if (ok) {
+    img.resize(npix);
+    ok = std::fread(img.data(), sizeof(float), npix, f) == static_cast<size_t>(npix);
+  }
+  std::fclose(f);
+  return ok;
+}
+
 int stream(const Options &o) {
   const auto t0 = std::chrono::steady_clock::now();
   const Sky sky = read_sky(o.sky);
+  // days an earlier run finished (--resume): their images go straight into the sum
+  std::vector<double> total(sky.npix, 0.0);
+  std::vector<int> todo;
+  int resumed = 0;
+  for (int k = 0; k < o.days; ++k) {
+    const int day = o.first_day + k;
+    std::vector<float> img;
+    if (o.resume && read_day_image(o.out_dir + "C" + std::to_string(day) + ".vimg", sky.npix, img)) {
+      for (int64_t j = 0; j < sky.npix; ++j) total[j] += std::isfinite(img[j]) ? img[j] : 0.0;
+      ++resumed;
+      continue;
+    }
+    todo.push_back(day);
+  }
   int ndev = 0;
-  cucall(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
-  ndev = std::max(1, std::min(ndev, std::min(o.max_devices, o.days)));
+  if (!todo.empty()) cucall(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  ndev = std::max(1, std::min(ndev, std::min(o.max_devices, static_cast<int>(todo.size()))));
   std::vector<std::vector<int>> mine(ndev);
-  for (int k = 0; k < o.days; ++k) mine[k % ndev].push_back(o.first_day + k);  // :279
+  for (size_t k = 0; k < todo.size(); ++k) mine[k % ndev].push_back(todo[k]);  // :279
   std::vector<std::vector<DayTiming>> timings(ndev);
-  std::vector<std::vector<double>> sums(ndev);
+  std::vector<std::vector<double>> sums(ndev, std::vector<double>(sky.npix, 0.0));
   std::vector<std::thread> threads;
-  for (int d = 0; d < ndev; ++d)
+  for (int d = 0; d < ndev && !todo.empty(); ++d)
     threads.emplace_back([&, d] { DevicePipeline(d, o, sky, mine[d]).run(timings[d], sums[d]); });
   for (auto &t : threads) t.join();
-  // day sum: per-device FP64 sums added in device order
-  std::vector<double> total(sky.npix, 0.0);
+  // day sum: the resumed days, then the per-device FP64 sums in device order
   for (int d = 0; d < ndev; ++d)
     for (int64_t j = 0; j < sky.npix; ++j) total[j] += sums[d][j];
   if (!o.sum_out.empty()) {
@@ -489,9 +525,10 @@ int stream(const Options &o) {
       gpu_ms += t.gpu_ms;
       rows += t.rows;
     }
-  std::printf("{\"days\": %d, \"devices\": %d, \"npix\": %lld, \"rows\": %lld, \"wall_s\": %.4f, "
-              "\"gpu_ms_total\": %.3f, \"per_day\": [%s]}\n",
-              o.days, ndev, static_cast<long long>(sky.npix), rows, wall, gpu_ms, per.c_str());
+  std::printf("{\"days\": %d, \"resumed_days\": %d, \"devices\": %d, \"npix\": %lld, "
+              "\"rows\": %lld, \"wall_s\": %.4f, \"gpu_ms_total\": %.3f, \"per_day\": [%s]}\n",
+              o.days, resumed, todo.empty() ? 0 : ndev, static_cast<long long>(sky.npix), rows, wall,
+              gpu_ms, per.c_str());
   return 0;
 }
 
@@ -576,6 +613,7 @@ int main(int argc, char **argv) {
     else if (a == "--frequency") o.frequency = std::atof(val("--frequency").c_str());
     else if (a == "--blockage") o.blockage = std::atoi(val("--blockage").c_str()) != 0;
     else if (a == "--fold-mirrors") o.fold = true;
+    else if (a == "--resume") o.resume = true;
     else if (a == "--fp64") o.fp64 = true;
     else if (a == "--out-dir") o.out_dir = val("--out-dir");
     else if (a == "--sum-out") o.sum_out = val("--sum-out");
@@ -601,5 +639,6 @@ int main(int argc, char **argv) {
   if (o.sky.empty() || o.days_dir.empty()) die("--sky and --days-dir are required");
   if (o.days < 1 || o.first_day < 1) die("--days and --first-day must be >= 1");
   if (!(o.frequency > 0)) die("--frequency must be > 0");
+  if (o.resume && o.out_dir.empty()) die("--resume needs --out-dir (the day images it resumes from)");
   return stream(o);
 }
