@@ -24,7 +24,7 @@ def _grads(p, x, d):
     d = d.clone().requires_grad_(True)
     L = reconstruct.loss(p, x, d)
     L.backward()
-    return float(L), x.grad.double(), d.grad.double()
+    return float(L.detach()), x.grad.double(), d.grad.double()
 
 
 def _oracle_loss(oracle, p, lmn, occ, x, d):

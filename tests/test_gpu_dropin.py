@@ -94,3 +94,26 @@ def test_noblockage_10m_reproduces_reference_output(tmp_path):
     ref_out = open(os.path.join(fix, "reference_stdout.txt")).read()
     np.testing.assert_allclose(viss_lines(stdout), viss_lines(ref_out), rtol=2e-5,
                                atol=2e-5 * np.abs(viss_lines(ref_out)).max())
+
+
+def test_malformed_inputs_end_with_a_message(tmp_path):
+    """Short or missing text inputs: a non-zero exit with a message naming the
+    problem (the reference reads missing files as zero rows and short ones as
+    garbage, vissgen3d_blockage.cu:216-237,317-326)."""
+    def call(*args):
+        return subprocess.run([os.path.join(BIN, "vissgen3d_blockage_10m"), *args], cwd=tmp_path,
+                              capture_output=True, text=True, timeout=300)
+    r = call()                                           # no earth_10Mhz/ at all
+    assert r.returncode != 0 and "cannot read npix" in r.stderr
+    case = refcase.make_case()
+    d = refcase.write_inputs(case, str(tmp_path), variant_10m=True)
+    lines = open(os.path.join(d, "theta_heal_10Mhz.txt")).read().splitlines()
+    open(os.path.join(d, "theta_heal_10Mhz.txt"), "w").write("\n".join(lines[:-5]) + "\n")
+    r = call()
+    assert r.returncode != 0 and "fewer than npix" in r.stderr
+    refcase.write_inputs(case, str(tmp_path), variant_10m=True)          # restore
+    rows = open(os.path.join(d, "bll1day1M.txt")).read().splitlines()
+    open(os.path.join(d, "bll1day1M.txt"), "w").write("\n".join(rows[:-7]) + "\n")
+    os.makedirs(tmp_path / "3dblockage10M", exist_ok=True)
+    r = call()
+    assert r.returncode != 0 and "fewer rows than uvw" in r.stderr

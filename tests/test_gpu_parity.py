@@ -190,6 +190,35 @@ def test_dcf_and_weights_bit_exact(viss, oracle, cuda_device):
     np.testing.assert_array_equal(c2.cpu().numpy().view(np.uint32), oracle.dcf(bll, 40000)[1])
 
 
+def test_dcf_and_weights_adversarial_values(viss, oracle, cuda_device):
+    """Shell edges, NaN/inf/negative/huge bll, |w| > bll, w = bll: the shell
+    index, counts, DCF, dg and clamped weight stay bit-equal to the oracle
+    (gs = -1 for NaN, saturated for huge values, clamped into [0, nr] when
+    indexing; dg = inf where |w/bll| >= 1, capped at 1/8 by the weight)."""
+    rng = np.random.default_rng(12)
+    bll = rng.uniform(0.0, 40.0, 4000).astype(np.float32)
+    w = (rng.uniform(-1, 1, 4000) * bll * 0.9).astype(np.float32)
+    edge = np.array([0.25, 0.75, 0.7500001, 1.25, np.nan, np.inf, -np.inf, -3.0, 0.0, 1e30,
+                     np.float32(2.0 ** 31), 5.0, 5.0, 5.0, 33.0], dtype=np.float32)
+    wedge = np.array([0.1, 0.5, 0.2, 1.25, 0.3, 1.0, 0.0, 1.0, 0.0, 2.0, 1.0, 5.0, -6.0, np.nan,
+                      -33.0], dtype=np.float32)
+    bll[:edge.size], w[:edge.size] = edge, wedge
+    nr = 70
+    for mult in (1, 2):
+        bt = torch.as_tensor(bll, device=cuda_device)
+        gs, counts, dcf = viss.dcf(bt, nr, multiplicity=mult)
+        ogs, ocounts, odcf = oracle.dcf(bll, nr, mult)
+        np.testing.assert_array_equal(gs.cpu().numpy(), ogs)
+        np.testing.assert_array_equal(counts.cpu().numpy().view(np.uint32), ocounts)
+        np.testing.assert_array_equal(dcf.cpu().numpy().view(np.uint32), odcf.view(np.uint32))
+        dg, wt = viss.weights(torch.as_tensor(w, device=cuda_device), bt, gs, dcf, nr)
+        odg = oracle.gamma_dg(w, bll)
+        np.testing.assert_array_equal(dg.cpu().numpy().view(np.uint32), odg.view(np.uint32))
+        np.testing.assert_array_equal(wt.cpu().numpy().view(np.uint32),
+                                      oracle.weights(ogs, odg, odcf, nr).view(np.uint32))
+    assert ogs[4] == -1
+
+
 def test_wrot_and_mirror(viss, oracle, cuda_device):
     rng = np.random.default_rng(6)
     n = 5000
