@@ -156,6 +156,30 @@ int viss_plan_tune(viss_plan *plan, const float *sky, const float *coef, float *
  * frequency per executable, vissgen3d_blockage.cu:568). */
 int viss_plan_set_channels(viss_plan *plan, int channels);
 
+/* ------------------------------------------------------- formation mode
+ * The samples of a satellite formation: for each of T snapshots, every pair
+ * a < b of its S satellites (lexicographic order; sample k = t * S(S-1)/2 +
+ * pair), with u = U[t][a] - U[t][b] (U: T x S x 3 FP64 wavelengths, e.g.
+ * (P - formation centre) / lambda).  The reference builds exactly these
+ * baselines (vissgen3d_blockage.cu:309-373 reads them per row); here the
+ * exponential factors per satellite, e^{-2 pi i u.s} = E_a conj(E_b), so a
+ * snapshot costs S exponentials per pixel instead of S(S-1)/2.  Same results
+ * as viss_forward / viss_adjoint with uvw = U_a - U_b, refs = (t S + a,
+ * t S + b, T S + t) and occ = [occ_sat; occ_snap] (split precision only).
+ *   off      T x S(S-1)/2 phase offsets in turns, or NULL
+ *   occ_sat  T x S x 4 occulter rows of the satellites (Moon), or NULL
+ *   occ_snap T x 4 rows of the snapshots (Earth cap), or NULL
+ * S must be 4, 6, 8 or 10.  Synchronises `stream` once.  No counterpart in the
+ * reference. */
+int viss_plan_set_formation(viss_plan *plan, int64_t T, int S, const double *U, const double *off,
+                            const double *occ_sat, const double *occ_snap, void *stream);
+/* V (T x S(S-1)/2 complex64) for sky (J FP32); flags VISS_NO_MASK, VISS_ACCUMULATE. */
+int viss_forward_formation(viss_plan *plan, const float *sky, float *V, int flags, void *stream);
+/* image (J FP32) = scale * the adjoint of the formation's samples for coef
+ * (T x S(S-1)/2 complex64); flags VISS_NO_MASK, VISS_ACCUMULATE. */
+int viss_adjoint_formation(viss_plan *plan, const float *coef, float *image, float scale, int flags,
+                           void *stream);
+
 /* Test hook for the failure path: the next viss_forward or viss_adjoint on
  * this plan has its first thread block skip the staging copy of its `tile`-th
  * tile (a pixel tile in the forward, a sample tile in the adjoint), so that

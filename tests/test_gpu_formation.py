@@ -1,0 +1,83 @@
+"""Formation mode (viss_plan_set_formation, csrc/formation.cu): every sample
+a pair of one snapshot's satellites, the exponential factored per satellite.
+Same arithmetic contract as the direct kernels: the forward and adjoint match
+the direct path on the same plan and the FP64 oracle (rel-L2 1e-5; masks from
+the same exact predicate), with Moon rows, Earth rows, phase offsets, no mask;
+invalid uses are rejected."""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from viss_optimize_3d_b200 import api, pipeline, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _case(cfg, f, dev, seed_off=None):
+    obs = synth.make_observation(cfg)
+    g = pipeline.upload(obs, f, device=dev)
+    U, occ_sat, occ_snap = pipeline.formation_inputs(obs, f, device=dev, occ=g.occ)
+    off = None
+    if seed_off is not None:
+        off = np.random.default_rng(seed_off).uniform(-3, 3, cfg.n_samples)
+        g.plan.set_samples(g.uvw, torch.as_tensor(off, device=dev), g.refs, g.occ)
+    g.plan.set_formation(U, None if off is None else off.reshape(cfg.n_snap, -1), occ_sat, occ_snap)
+    return obs, g, off
+
+
+@pytest.mark.parametrize("cfgname,f,S,nside,T,with_off", [
+    ("c2", 1e7, 8, 16, 30, False),
+    ("c3_10mhz", 1e7, 10, 16, 24, True),
+    ("c3_1mhz", 1e6, 10, 32, 16, False),
+])
+def test_formation_matches_direct_and_oracle(oracle, cuda_device, cfgname, f, S, nside, T, with_off):
+    cfg = synth.scaled(synth.CONFIGS[cfgname], nside=nside, n_snap=T, n_sat=S)
+    obs, g, off = _case(cfg, f, cuda_device, seed_off=3 if with_off else None)
+    lmn, uvw = g.lmn.cpu().numpy(), g.uvw.cpu().numpy()
+    occ = g.occ.cpu().numpy() if g.occ is not None else None
+    Vd = g.plan.forward(g.sky).cpu().numpy().astype(np.complex128)
+    Vf = g.plan.forward_formation(g.sky).cpu().numpy().astype(np.complex128)
+    Vo = oracle.forward(uvw, lmn, g.sky.cpu().numpy().astype(np.float64), obs.refs, occ, off=off)
+    assert rel_l2(Vf, Vo) <= 1e-5, rel_l2(Vf, Vo)
+    assert rel_l2(Vf, Vd) <= 1e-5, rel_l2(Vf, Vd)
+    rng = np.random.default_rng(5)
+    a = (rng.standard_normal(cfg.n_samples) + 1j * rng.standard_normal(cfg.n_samples)).astype(np.complex64)
+    at = torch.as_tensor(a, device=cuda_device)
+    Cd = g.plan.adjoint(at, scale=2.0).cpu().numpy()
+    Cf = g.plan.adjoint_formation(at, scale=2.0).cpu().numpy()
+    Co = 2.0 * oracle.adjoint(uvw, a.astype(np.complex128), lmn, obs.refs, occ, off=off)
+    assert rel_l2(Cf, Co) <= 1e-5, rel_l2(Cf, Co)
+    assert rel_l2(Cf, Cd) <= 1e-5, rel_l2(Cf, Cd)
+    # without the mask
+    Vn = g.plan.forward_formation(g.sky, mask=False).cpu().numpy().astype(np.complex128)
+    Von = oracle.forward(uvw, lmn, g.sky.cpu().numpy().astype(np.float64), off=off)
+    assert rel_l2(Vn, Von) <= 1e-5, rel_l2(Vn, Von)
+    Cn = g.plan.adjoint_formation(at, mask=False).cpu().numpy()
+    Con = oracle.adjoint(uvw, a.astype(np.complex128), lmn, off=off)
+    assert rel_l2(Cn, Con) <= 1e-5, rel_l2(Cn, Con)
+
+
+def test_formation_rejects_invalid_use(cuda_device):
+    from viss_optimize_3d_b200._capi import VissError, check, lib
+    lmn = api.pix2lmn(4, "ring", device=cuda_device)
+    plan = api.Plan(lmn)
+    with pytest.raises(VissError, match="formation not set"):
+        plan.form_T, plan.form_B = 1, 1
+        plan.forward_formation(torch.ones(lmn.shape[0], device=cuda_device))
+    with pytest.raises(VissError, match="S must be"):
+        plan.set_formation(torch.zeros((3, 7, 3), dtype=torch.float64))
+    plan.set_formation(torch.zeros((3, 4, 3), dtype=torch.float64))
+    V = torch.empty(18, dtype=torch.complex64, device=cuda_device)
+    sky = torch.ones(lmn.shape[0], device=cuda_device)
+    with pytest.raises(VissError, match="split precision only"):
+        check(lib.viss_forward_formation(plan._h, sky.data_ptr(), V.data_ptr(), 1, None), "fwd")
+    U = torch.zeros((3, 4, 3), dtype=torch.float64)
+    U[1, 2, 0] = float("nan")
+    with pytest.raises(VissError, match="non-finite"):
+        plan.set_formation(U)

@@ -24,7 +24,7 @@ LIB = os.path.join(PKG, "libviss.so")
 BIN = os.path.join(PKG, "bin")
 
 CU_SOURCES = ["healpix.cu", "geometry.cu", "visibility.cu", "dcf.cu", "capi.cu", "noalloc.cu",
-              "days.cu"]
+              "days.cu", "formation.cu"]
 HEADERS = ["viss_common.cuh", "visibility.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -223,6 +223,59 @@ class Plan:
                                self._flags(fp64, mask, use_offset), _stream(coef)), "viss_adjoint")
         return out
 
+    # ---------------------------------------------------- formation mode
+    def set_formation(self, U, off=None, occ_sat=None, occ_snap=None):
+        """Samples of a satellite formation (viss_plan_set_formation): U is
+        (T, S, 3) FP64 satellite vectors in wavelengths; sample k = t * B + pair
+        for the B = S(S-1)/2 pairs a < b in lexicographic order, u = U_a - U_b.
+        off (T, B) turns, occ_sat (T, S, 4) and occ_snap (T, 4) occulter rows,
+        each optional.  Kept beside the plan's ordinary samples."""
+        U = torch.as_tensor(U) if not isinstance(U, torch.Tensor) else U
+        if U.dim() != 3 or U.shape[2] != 3:
+            raise ValueError("U must be (T, S, 3)")
+        T, S = int(U.shape[0]), int(U.shape[1])
+        B = S * (S - 1) // 2
+        U = _cuda(U.reshape(T * S, 3), torch.float64, self.device, shape_last=3)
+        off = _cuda(None if off is None else torch.as_tensor(off).reshape(T * B), torch.float64, self.device)
+        occ_sat = _cuda(None if occ_sat is None else torch.as_tensor(occ_sat).reshape(T * S, 4),
+                        torch.float64, self.device, shape_last=4)
+        occ_snap = _cuda(occ_snap, torch.float64, self.device, shape_last=4)
+        check(lib.viss_plan_set_formation(self._h, T, S, _p(U), _p(off), _p(occ_sat), _p(occ_snap),
+                                          _stream(U)), "viss_plan_set_formation")
+        self.form_T, self.form_S, self.form_B = T, S, B
+
+    def forward_formation(self, sky, mask: bool = True, out: torch.Tensor | None = None):
+        """V (T * B complex64) of the formation's samples."""
+        sky = _cuda(sky, torch.float32, self.device)
+        if sky.numel() != self.J:
+            raise ValueError(f"sky must hold {self.J} values")
+        n = self.form_T * self.form_B
+        if out is None:
+            out = torch.empty(n, dtype=torch.complex64, device=self.device)
+        elif (out.dtype != torch.complex64 or not out.is_contiguous() or out.numel() != n
+              or out.device != self.device):
+            raise ValueError(f"out must be a contiguous complex64 tensor of {n} values on {self.device}")
+        check(lib.viss_forward_formation(self._h, _p(sky), _p(out), 0 if mask else capi.VISS_NO_MASK,
+                                         _stream(sky)), "viss_forward_formation")
+        return out
+
+    def adjoint_formation(self, coef, scale: float = 1.0, mask: bool = True,
+                          out: torch.Tensor | None = None):
+        """img (J FP32) = scale * the adjoint of the formation's samples."""
+        n = self.form_T * self.form_B
+        coef = _cuda(coef, torch.complex64, self.device)
+        if coef.shape != (n,):
+            raise ValueError(f"coef must have shape ({n},)")
+        if out is None:
+            out = torch.empty(self.J, dtype=torch.float32, device=self.device)
+        elif (out.dtype != torch.float32 or not out.is_contiguous() or out.numel() != self.J
+              or out.device != self.device):
+            raise ValueError(f"out must be a contiguous float32 tensor of {self.J} values on {self.device}")
+        check(lib.viss_adjoint_formation(self._h, _p(coef), _p(out), float(scale),
+                                         0 if mask else capi.VISS_NO_MASK, _stream(coef)),
+              "viss_adjoint_formation")
+        return out
+
     def last_counts(self):
         """(exponentials evaluated, K*J) of the last forward/adjoint (syncs)."""
         ev, tot = C.c_int64(), C.c_int64()

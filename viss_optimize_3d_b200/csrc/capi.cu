@@ -33,6 +33,12 @@ cudaError_t sort_pixel_keys(long long, unsigned long long *, unsigned long long 
 cudaError_t launch_stage_pixels(long long, long long, const double *, const int *, double4 *,
                                 float4 *, cudaStream_t);
 cudaError_t launch_occ32(long long, const double4 *, float4 *, cudaStream_t);
+cudaError_t launch_form_stage(long long, int, const double *, const double *, double4 *,
+                              unsigned long long *, cudaStream_t);
+cudaError_t launch_form_stage_coef(long long, int, const float2 *, const double *, float2 *,
+                                   cudaStream_t);
+cudaError_t launch_form_reduce_fwd(long long, int, const double2 *, const double *, float2 *, int,
+                                   cudaStream_t);
 cudaError_t launch_stage_sky(long long, long long, const double4 *, const int *, const float *,
                              float, double4 *, int, cudaStream_t);
 cudaError_t launch_stage_coef(long long, long long, const float2 *, float2 *, cudaStream_t);
@@ -128,6 +134,16 @@ struct viss_plan {
   long long G = 0;
   float2 *coef = nullptr;  size_t coef_cap = 0;
   double max_turns = 0;
+  // satellite-formation mode (viss_plan_set_formation)
+  long long form_T = 0;
+  int form_S = 0;
+  double4 *form_U = nullptr;    size_t form_U_cap = 0;
+  double *form_off = nullptr;   size_t form_off_cap = 0;
+  bool form_has_off = false;
+  double4 *form_occ = nullptr;  size_t form_occ_cap = 0;   // [T*S satellites][T snapshots]
+  float4 *form_occ32 = nullptr; size_t form_occ32_cap = 0;
+  int form_sat = 0, form_snap = 0;
+  float2 *form_coef = nullptr;  size_t form_coef_cap = 0;
   // workspace + device status words
   void *part = nullptr;    size_t part_cap = 0;
   // [0] terms evaluated, [1] error flags, [2] terms evaluated in mixed tiles,
@@ -310,8 +326,10 @@ int viss_plan_create(viss_plan **plan) {
 
 int viss_plan_destroy(viss_plan *p) {
   if (!p) return VISS_OK;
-  void *bufs[] = {p->pix,  p->pixsky, p->cones, p->perm, p->samp,     p->refs,
-                  p->occ,  p->occ32,  p->coef,  p->part, p->dev_words};
+  void *bufs[] = {p->pix,    p->pixsky,  p->cones,    p->perm,      p->samp,
+                  p->refs,   p->occ,     p->occ32,    p->coef,      p->part,
+                  p->dev_words, p->form_U, p->form_off, p->form_occ, p->form_occ32,
+                  p->form_coef};
   for (void *b : bufs)
     if (b) cudaFree(b);
   delete p;
@@ -566,6 +584,148 @@ int viss_plan_set_channels(viss_plan *p, int channels) {
   if (channels > 65535) return fail(VISS_ERR_ARG, "viss_plan_set_channels: at most 65535 channels");
   p->channels = channels;
   p->Kc = Kc;
+  return VISS_OK;
+}
+
+// -------------------------------------------------------- formation mode
+int viss_plan_set_formation(viss_plan *p, int64_t T, int S, const double *U, const double *off,
+                            const double *occ_sat, const double *occ_snap, void *stream) {
+  if (!p || T < 1 || !U) return fail(VISS_ERR_ARG, "viss_plan_set_formation: bad arguments");
+  if (S != 4 && S != 6 && S != 8 && S != 10)
+    return fail(VISS_ERR_ARG, "viss_plan_set_formation: S must be 4, 6, 8 or 10 satellites");
+  const long long B = viss::form_pairs(S);
+  if (T * B >= (1LL << 31)) return fail(VISS_ERR_ARG, "viss_plan_set_formation: too many samples");
+  const cudaStream_t st = as_stream(stream);
+  const long long rows = T * S + T;
+  p->form_T = 0;  // not usable until staged and checked
+  if (int s = ensure(p->form_U, p->form_U_cap, sizeof(double4) * T * S, "formation vectors")) return s;
+  if (int s = ensure(p->form_occ, p->form_occ_cap, sizeof(double4) * rows, "formation occulters"))
+    return s;
+  if (int s = ensure(p->form_occ32, p->form_occ32_cap, sizeof(float4) * rows, "formation occulters"))
+    return s;
+  if (off && (ensure(p->form_off, p->form_off_cap, sizeof(double) * T * B, "formation offsets")))
+    return VISS_ERR_ALLOC;
+  VISS_CUDA(cudaMemsetAsync(p->form_occ, 0, sizeof(double4) * rows, st), "viss_plan_set_formation");
+  if (occ_sat)
+    VISS_CUDA(cudaMemcpyAsync(p->form_occ, occ_sat, sizeof(double4) * T * S, cudaMemcpyDeviceToDevice, st),
+              "viss_plan_set_formation: satellite rows");
+  if (occ_snap)
+    VISS_CUDA(cudaMemcpyAsync(p->form_occ + T * S, occ_snap, sizeof(double4) * T,
+                              cudaMemcpyDeviceToDevice, st),
+              "viss_plan_set_formation: snapshot rows");
+  VISS_CUDA(viss::launch_occ32(rows, p->form_occ, p->form_occ32, st), "viss_plan_set_formation");
+  if (off)
+    VISS_CUDA(cudaMemcpyAsync(p->form_off, off, sizeof(double) * T * B, cudaMemcpyDeviceToDevice, st),
+              "viss_plan_set_formation: offsets");
+  VISS_CUDA(cudaMemsetAsync(p->dev_words + 3, 0, sizeof(unsigned long long), st), "viss_plan_set_formation");
+  VISS_CUDA(viss::launch_form_stage(T, S, U, off, p->form_U, p->dev_words + 3, st), "viss_plan_set_formation");
+  unsigned long long bits = 0;
+  VISS_CUDA(cudaMemcpyAsync(&bits, p->dev_words + 3, sizeof(bits), cudaMemcpyDeviceToHost, st),
+            "viss_plan_set_formation: bound");
+  VISS_CUDA(cudaStreamSynchronize(st), "viss_plan_set_formation: sync");
+  double bound;
+  std::memcpy(&bound, &bits, sizeof(bound));
+  if (!std::isfinite(bound))
+    return fail(VISS_ERR_NOTFINITE, "viss_plan_set_formation: non-finite satellite vectors or offsets");
+  if (!(bound < viss::kMaxTurns))
+    return fail(VISS_ERR_ARG, "viss_plan_set_formation: |U| or |off| exceeds 2^28 turns");
+  p->form_T = T;
+  p->form_S = S;
+  p->form_has_off = off != nullptr;
+  p->form_sat = occ_sat != nullptr;
+  p->form_snap = occ_snap != nullptr;
+  return VISS_OK;
+}
+
+static int check_formation(viss_plan *p, const void *in, const void *out, int flags, const char *who) {
+  if (!p || !in || !out) return fail(VISS_ERR_ARG, std::string(who) + ": bad arguments");
+  if (p->J <= 0 || p->form_T <= 0)
+    return fail(VISS_ERR_STATE, std::string(who) + ": pixels or formation not set");
+  if (flags & VISS_FP64)
+    return fail(VISS_ERR_ARG, std::string(who) + ": split precision only (use viss_forward / viss_adjoint for FP64)");
+  return VISS_OK;
+}
+
+static viss::FormParams form_params(viss_plan *p, int flags) {
+  const bool masked = !(flags & VISS_NO_MASK);
+  viss::FormParams fp{};
+  fp.U = p->form_U;
+  fp.occ = p->form_occ;
+  fp.occ32 = p->form_occ32;
+  fp.sat_rows = masked && p->form_sat;
+  fp.snap_rows = masked && p->form_snap;
+  fp.cones = p->cones;
+  fp.ntiles = p->ntiles;
+  fp.Jpad = p->Jpad;
+  fp.T = p->form_T;
+  fp.counter = p->dev_words;
+  fp.err = reinterpret_cast<int *>(p->dev_words + 1);
+  return fp;
+}
+
+int viss_forward_formation(viss_plan *p, const float *sky, float *V, int flags, void *stream) {
+  if (int s = check_formation(p, sky, V, flags, "viss_forward_formation")) return s;
+  const NvtxRange range("viss_forward_formation");
+  const cudaStream_t st = as_stream(stream);
+  const long long T = p->form_T, B = viss::form_pairs(p->form_S);
+  // about 16 waves of one block per SM, each block 8 snapshots x a chunk of tiles
+  const long long blocks = (T + viss::kFormNT / 32 - 1) / (viss::kFormNT / 32);
+  long long c = (16LL * p->nsm + blocks - 1) / blocks;
+  c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 4)));
+  viss::FormParams fp = form_params(p, flags);
+  fp.tiles_per_chunk = static_cast<int>((p->ntiles + c - 1) / c);
+  const int nchunk = (p->ntiles + fp.tiles_per_chunk - 1) / fp.tiles_per_chunk;
+  fp.nchunk = nchunk;
+  if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * T * B)) return s;
+  if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * p->Jpad, "pixel+sky records")) return s;
+  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, 1, st),
+            "viss_forward_formation: sky");
+  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_forward_formation");
+  fp.pix = p->pixsky;
+  fp.part_fwd = static_cast<double2 *>(p->part);
+  VISS_CUDA(viss::launch_form_forward(fp, p->form_S, nchunk, st), "viss_forward_formation: kernel");
+  VISS_CUDA(viss::launch_form_reduce_fwd(T * B, nchunk, fp.part_fwd, p->form_has_off ? p->form_off : nullptr,
+                                         reinterpret_cast<float2 *>(V), (flags & VISS_ACCUMULATE) ? 1 : 0, st),
+            "viss_forward_formation: reduce");
+  p->last_total = T * B * p->J;
+  p->last_stream = st;
+  return VISS_OK;
+}
+
+int viss_adjoint_formation(viss_plan *p, const float *coef, float *image, float scale, int flags,
+                           void *stream) {
+  if (int s = check_formation(p, coef, image, flags, "viss_adjoint_formation")) return s;
+  const NvtxRange range("viss_adjoint_formation");
+  const cudaStream_t st = as_stream(stream);
+  const long long T = p->form_T, B = viss::form_pairs(p->form_S);
+  const int CB = viss::form_coef_stride(p->form_S);
+  if (int s = ensure(p->form_coef, p->form_coef_cap, sizeof(float2) * T * CB, "formation coefficients"))
+    return s;
+  VISS_CUDA(viss::launch_form_stage_coef(T, p->form_S, reinterpret_cast<const float2 *>(coef),
+                                         p->form_has_off ? p->form_off : nullptr, p->form_coef, st),
+            "viss_adjoint_formation: coefficients");
+  const long long per = viss::form_adjoint_pixels_per_block();
+  const long long blocks = (p->Jpad + per - 1) / per;
+  long long c = (16LL * p->nsm + blocks - 1) / blocks;
+  const long long max_c = std::max<long long>(1, (T + 4 * viss::kFormSnapTile - 1) / (4 * viss::kFormSnapTile));
+  c = std::max<long long>(1, std::min(c, std::min<long long>(max_c, 65535)));
+  long long spc = (T + c - 1) / c;
+  spc = (spc + viss::kFormSnapTile - 1) / viss::kFormSnapTile * viss::kFormSnapTile;
+  const int nchunk = static_cast<int>((T + spc - 1) / spc);
+  if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->Jpad)) return s;
+  VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_adjoint_formation");
+  viss::FormParams fp = form_params(p, flags);
+  fp.pix = p->pix;
+  fp.snaps_per_chunk = static_cast<int>(spc);
+  fp.nchunk = nchunk;
+  fp.coef = p->form_coef;
+  fp.part_adj = static_cast<double *>(p->part);
+  VISS_CUDA(viss::launch_form_adjoint(fp, p->form_S, nchunk, st), "viss_adjoint_formation: kernel");
+  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, 1, fp.part_adj, p->perm, scale, image,
+                                    (flags & VISS_ACCUMULATE) ? 1 : 0, st),
+            "viss_adjoint_formation: reduce");
+  p->last_total = T * B * p->J;
+  p->last_stream = st;
   return VISS_OK;
 }
 

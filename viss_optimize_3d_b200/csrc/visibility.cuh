@@ -51,6 +51,39 @@ struct AdjParams {
   int drop_tile;                // test hook: CTA (0, 0) skips this tile's copy (-1: none)
 };
 
+// Satellite-formation mode (formation.cu): every sample is a pair a < b of the
+// S satellites of one snapshot (lexicographic pair order, samples t-major),
+// u = U[t][a] - U[t][b].
+constexpr int kFormNT = 256;       // threads per block (both kernels)
+constexpr int kFormSnapTile = 8;   // snapshots per adjoint staging tile
+constexpr int kFormFoldTiles = 32; // forward: pixel tiles between FP64 folds
+__host__ __device__ constexpr int form_pairs(int S) { return S * (S - 1) / 2; }
+__host__ __device__ constexpr int form_coef_stride(int S) { return (form_pairs(S) + 1) & ~1; }
+
+struct FormParams {
+  const double4 *U;       // [T][S] satellite vectors in wavelengths (.w unused)
+  const double4 *occ;     // exact rows: [T*S] satellites, then [T] snapshots
+  const float4 *occ32;    // the same, classification rows
+  int sat_rows, snap_rows;  // 1 if those rows are present (and masking is on)
+  const double4 *pix;     // forward: pixel + sky records; adjoint: pixel records [Jpad]
+  const float4 *cones;    // tile cones (cone_count layout)
+  int ntiles;
+  long long Jpad;
+  long long T;
+  int tiles_per_chunk;    // forward
+  int snaps_per_chunk;    // adjoint, a multiple of kFormSnapTile
+  int nchunk;
+  const float2 *coef;     // adjoint: [T][form_coef_stride(S)] coefficients, offsets applied
+  double2 *part_fwd;      // [chunk][T * B]
+  double *part_adj;       // [chunk][Jpad]
+  unsigned long long *counter;
+  int *err;
+};
+
+cudaError_t launch_form_forward(const FormParams &p, int S, int nchunk, cudaStream_t st);
+cudaError_t launch_form_adjoint(const FormParams &p, int S, int nchunk, cudaStream_t st);
+int form_adjoint_pixels_per_block();
+
 struct FwdShape { int R, minb; };
 struct AdjShape { int P, minb; };
 constexpr int kNumFwdShapes = 4;

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import api
-from .synth import Observation, R_MOON
+from .synth import C_LIGHT, Observation, R_MOON
 
 
 @dataclasses.dataclass
@@ -51,6 +51,25 @@ def build_occulters(obs: Observation, device) -> torch.Tensor | None:
     if obs.earth_rows is not None:
         occ = torch.cat([occ, torch.as_tensor(obs.earth_rows, dtype=torch.float64, device=device)])
     return occ.contiguous()
+
+
+def formation_inputs(obs: Observation, f_hz: float, device="cuda", occ: torch.Tensor | None = None):
+    """(U, occ_sat, occ_snap) of viss_plan_set_formation for a synthetic
+    observation: U = (P - formation centre) / lambda per snapshot (the pair
+    differences are the observation's uvw), and the occulter rows split into
+    the satellites' (T*S first rows of build_occulters) and the snapshots'."""
+    cfg = obs.cfg
+    P = np.asarray(obs.positions, dtype=np.float64)
+    U = (P - P.mean(axis=1, keepdims=True)) / (C_LIGHT / f_hz)
+    occ_sat = occ_snap = None
+    if obs.refs is not None:
+        occ = build_occulters(obs, device) if occ is None else occ
+        T, S = cfg.n_snap, cfg.n_sat
+        if cfg.moon:
+            occ_sat = occ[:T * S].reshape(T, S, 4)
+        if obs.earth_rows is not None:
+            occ_snap = occ[T * S:T * S + T]
+    return torch.as_tensor(U, device=device), occ_sat, occ_snap
 
 
 def upload(obs: Observation, f_hz: float, device="cuda", lmn: torch.Tensor | None = None,
