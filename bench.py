@@ -131,6 +131,8 @@ def run_ours(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    if args.formation:
+        return run_formation(args, rank, world, local_rank)
     if args.workload == "c3_small":
         cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
     else:
@@ -331,6 +333,160 @@ def run_ours(args, rank, world, local_rank):
     }
     if args.cpu_baseline:
         res["cpu_baseline"] = cpu_baseline(obs, f_hz, budget_s=args.cpu_seconds)
+    return res
+
+
+# ------------------------------------------------------ formation mode
+FORM_FFMA_PER_TERM = 4   # one complex multiply-accumulate G_a conj(F_b) per (pair, pixel)
+
+
+def run_formation(args, rank, world, local_rank):
+    """The same step through the formation entry points: the samples given as
+    satellite vectors U (T x S x 3), S exponentials per pixel and snapshot,
+    the S(S-1)/2 pair sums as FP32 complex multiply-accumulates."""
+    import numpy as np
+    import torch
+    from viss_optimize_3d_b200 import api, pipeline, replicas, synth
+    from viss_optimize_3d_b200._capi import check, lib
+    import ctypes as C
+
+    dev = torch.device("cuda", local_rank)
+    if args.workload == "c3_small":
+        cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
+    elif args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz"):
+        cfg = synth.CONFIGS[args.workload]
+    else:
+        raise SystemExit(f"--formation covers the single-channel workloads, not {args.workload}")
+    if world > 1:
+        import dataclasses
+        day = replicas.days_for_rank(world, rank, world)[0]
+        cfg = dataclasses.replace(cfg, day=float(day - 1))
+    f_hz = cfg.freqs_hz[0]
+    obs = synth.make_observation(cfg)
+    g = pipeline.upload(obs, f_hz, device=dev)
+    U, occ_sat, occ_snap = pipeline.formation_inputs(obs, f_hz, device=dev, occ=g.occ)
+    plan = g.plan
+    plan.set_formation(U, None, occ_sat, occ_snap)
+    K, J = plan.form_T * plan.form_B, plan.J
+    terms_per_step = 2 * K * J
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def image(V):
+        gs, _c, dcf = api.dcf(g.bll, g.nr, multiplicity=2)
+        _dg, wt = api.weights(g.w, g.bll, gs, dcf, g.nr)
+        return plan.adjoint_formation(api.scale_coef(wt, V), scale=2.0, mask=cfg.imaging_mask)
+
+    for _ in range(args.warmup):
+        image(plan.forward_formation(g.sky))
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        ev[i][0].record(stream)
+        V = plan.forward_formation(g.sky)
+        ev[i][1].record(stream)
+        gs, _c, dcf = api.dcf(g.bll, g.nr, multiplicity=2)
+        _dg, wt = api.weights(g.w, g.bll, gs, dcf, g.nr)
+        coef = api.scale_coef(wt, V)
+        ev[i][2].record(stream)
+        plan.adjoint_formation(coef, scale=2.0, mask=cfg.imaging_mask)
+        ev[i][3].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        torch.distributed.barrier()
+    total_s = sum(e[0].elapsed_time(e[3]) for e in ev) / 1e3
+    fwd_s = statistics.mean(e[0].elapsed_time(e[1]) for e in ev) / 1e3
+    adj_s = statistics.mean(e[2].elapsed_time(e[3]) for e in ev) / 1e3
+    plan.forward_formation(g.sky)
+    ev_f, _mx, tot = plan.last_stats()
+    plan.adjoint_formation(coef, scale=2.0, mask=cfg.imaging_mask)
+    ev_a, _mx, _ = plan.last_stats()
+    # parity of this step against the direct kernels on the same plan
+    Vd = plan.forward(g.sky).to(torch.complex128)
+    Vf = plan.forward_formation(g.sky).to(torch.complex128)
+    rel_v = (torch.linalg.norm(Vf - Vd) / torch.linalg.norm(Vd)).item()
+
+    # end to end: pinned host sky and satellite vectors -> image and V on the host
+    sky_h = torch.from_numpy(obs.sky_at(f_hz).astype(np.float32) * np.float32(4 * math.pi / J)).pin_memory()
+    U_h = U.cpu().pin_memory()
+    U_d, sky_d = torch.empty_like(U), torch.empty_like(g.sky)
+    img_h = torch.empty(J, dtype=torch.float32).pin_memory()
+    V_h = torch.empty(K, dtype=torch.complex64).pin_memory()
+    os_p = C.c_void_p(occ_sat.data_ptr()) if occ_sat is not None else None
+    on_p = C.c_void_p(occ_snap.data_ptr()) if occ_snap is not None else None
+
+    def e2e_step():
+        sky_d.copy_(sky_h, non_blocking=True)
+        U_d.copy_(U_h, non_blocking=True)
+        check(lib.viss_plan_set_formation(plan._h, plan.form_T, plan.form_S, C.c_void_p(U_d.data_ptr()),
+                                          None, os_p, on_p, C.c_void_p(stream.cuda_stream)),
+              "viss_plan_set_formation")
+        Vd_ = plan.forward_formation(sky_d)
+        imgd = image(Vd_)
+        V_h.copy_(Vd_, non_blocking=True)
+        img_h.copy_(imgd, non_blocking=True)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = e0.elapsed_time(e1) / 1e3
+    total_s, e2e_s = replicas.max_over_ranks([total_s, e2e_s], device=dev)
+    if rank != 0:
+        return None
+    pk, pk_kind = peaks()
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_terms = 128 / FORM_FFMA_PER_TERM * nsm * pk["sm_max_mhz"] * 1e6
+    dom = "forward" if fwd_s >= adj_s else "adjoint"
+    dom_s = max(fwd_s, adj_s)
+    dom_eval = ev_f if dom == "forward" else ev_a
+    achieved = K * J / dom_s
+    res = {
+        "metric": METRIC,
+        "value": round(terms_per_step * args.steps * world / total_s / 1e9, 3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_s / args.steps * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64-phase/f32-sincos/f32-pair-products",
+        "data": "synthetic (seeded lunar-orbit formation and log-normal sky, see synth.py)",
+        "config": {"workload": WORKLOAD_TEXT.get(args.workload, args.workload) + "; formation mode",
+                   "pixels": J, "samples": K, "satellites": plan.form_S, "snapshots": plan.form_T,
+                   "terms_per_step": terms_per_step, "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": round(terms_per_step * e2e_steps / e2e_s / 1e9 * world, 3), "unit": UNIT,
+                "h2d_bytes_per_step": J * 4 + U.numel() * 8, "d2h_bytes_per_step": J * 4 + K * 8,
+                "path": "pinned host sky/U -> viss_plan_set_formation -> viss_forward_formation -> "
+                        "viss_dcf/viss_weights -> viss_adjoint_formation -> pinned host V/image"},
+        "roofline": {"bound": "fp32", "kernel": f"k_form_{dom}",
+                     "achieved": round(achieved / 1e9, 2), "peak": round(peak_terms / 1e9, 1),
+                     "unit": "Gterms/s", "frac": round(achieved / peak_terms, 4),
+                     "peak_source": f"128 FP32 lanes/clk/SM / {FORM_FFMA_PER_TERM} FFMA per term x {nsm} SMs "
+                                    f"x sm_max_mhz ({pk_kind})",
+                     "evaluated_frac": round(dom_eval / (K * J), 4), "traffic": None},
+        "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
+        "forward_rel_l2_vs_direct": float(f"{rel_v:.3e}"),
+        "gpu_launches": 10 * args.steps,
+        "clocks": clk,
+    }
     return res
 
 
@@ -669,6 +825,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOAD_TEXT),
                     help="benchmark configuration (default: the headline one)")
+    ap.add_argument("--formation", action="store_true",
+                    help="run the step through the formation entry points (satellite vectors)")
     ap.add_argument("--stream-days", type=int, default=4,
                     help="days of the stream workload")
     args = ap.parse_args()

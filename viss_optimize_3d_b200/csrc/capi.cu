@@ -669,7 +669,7 @@ int viss_forward_formation(viss_plan *p, const float *sky, float *V, int flags, 
   const cudaStream_t st = as_stream(stream);
   const long long T = p->form_T, B = viss::form_pairs(p->form_S);
   // about 16 waves of one block per SM, each block 8 snapshots x a chunk of tiles
-  const long long blocks = (T + viss::kFormNT / 32 - 1) / (viss::kFormNT / 32);
+  const long long blocks = (T + viss::kFormFwdNT / 32 - 1) / (viss::kFormFwdNT / 32);
   long long c = (16LL * p->nsm + blocks - 1) / blocks;
   c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 4)));
   viss::FormParams fp = form_params(p, flags);

@@ -80,7 +80,14 @@ __device__ __forceinline__ void classify(const float4 &cone, const float4 *row32
 // FP32 sums cover at most kFormFoldTiles * 4 = 128 pixels; they are then
 // summed over the warp and added to FP64 accumulators (lane l keeps pairs l,
 // l + 32, l + 64).
-template <int S, bool MIX>
+//
+// Tile modes (warp-uniform, from the classification): kOpen -- every row sees
+// the whole tile, no mask arithmetic; kMixed -- the general case: satellites
+// that see none of it are zeroed by a uniform factor, rows that see part of
+// it take the exact per-pixel predicate.
+enum FormMode { kOpen = 0, kMixed = 1 };
+
+template <int S, int MODE>
 __device__ __forceinline__ void form_fwd_tile(const double4 *tp, const double4 *U,
                                               const double4 *rows, unsigned hid, unsigned mix,
                                               float (&ar)[form_pairs(S)],
@@ -91,15 +98,19 @@ __device__ __forceinline__ void form_fwd_tile(const double4 *tp, const double4 *
     const double4 rec = tp[q * 32 + lane];
     const double x = rec.x, y = rec.y, z = rec.z;
     float I = sky_bits(rec);
-    if (MIX && ((mix >> S) & 1u)) I = visible_row(rows[S], x, y, z) ? I : 0.f;
+    if (MODE == kMixed && ((mix >> S) & 1u)) I = visible_row(rows[S], x, y, z) ? I : 0.f;
     float Gr[S - 1], Gi[S - 1];
 #pragma unroll
     for (int b = 0; b < S; ++b) {
       float c, s;
       sat_exp(U[b], x, y, z, c, s);
-      float m = ((hid >> b) & 1u) ? 0.f : 1.f;
-      if (MIX && ((mix >> b) & 1u)) m = visible_row(rows[b], x, y, z) ? m : 0.f;
-      const float Fr = m * c, Fi = -m * s;   // F_b = m e^{-i theta}
+      float Fr = c, Fi = -s;                 // F_b = m e^{-i theta}
+      if (MODE != kOpen) {
+        float m = ((hid >> b) & 1u) ? 0.f : 1.f;
+        if (MODE == kMixed && ((mix >> b) & 1u)) m = visible_row(rows[b], x, y, z) ? m : 0.f;
+        Fr *= m;
+        Fi *= m;
+      }
       const float cr = Fr, ci = -Fi;         // conj(F_b)
 #pragma unroll
       for (int a = 0; a < b; ++a) {
@@ -116,9 +127,9 @@ __device__ __forceinline__ void form_fwd_tile(const double4 *tp, const double4 *
 }
 
 template <int S>
-__global__ void __launch_bounds__(kFormNT, 1) k_form_forward(const FormParams p) {
+__global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams p) {
   constexpr int B = form_pairs(S);
-  constexpr int NW = kFormNT / 32;
+  constexpr int NW = kFormFwdNT / 32;
   constexpr int ST = kFwdStages;
   __shared__ __align__(128) double4 s_pix[ST][kTilePix];
   __shared__ __align__(16) double4 s_U[NW][S];
@@ -206,8 +217,8 @@ __global__ void __launch_bounds__(kFormNT, 1) k_form_forward(const FormParams p)
     }
     // a pair needs both satellites: skip the tile unless two see some of it
     if (tok && !snap_hidden && S - __popc(hid) >= 2) {
-      if (mix) form_fwd_tile<S, true>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
-      else form_fwd_tile<S, false>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
+      if (mix | hid) form_fwd_tile<S, kMixed>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
+      else form_fwd_tile<S, kOpen>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
       evaluated += static_cast<unsigned long long>(kTilePix) * B;
     }
     ring_release(s_empty, stage);
@@ -246,11 +257,71 @@ struct FormAdjStage {
   float2 coef[kFormSnapTile * form_coef_stride(S)];
 };
 
+// Q[q] (one snapshot) for the lane's P pixels; cf is the snapshot's column
+// layout of coefficients (form_col0), U its satellite vectors.
+template <int S, int P, int MODE>
+__device__ __forceinline__ void form_adj_snapshot(const double4 *U, const float2 *cf,
+                                                  const double4 *rows, unsigned hid, unsigned mix,
+                                                  const double (&sx)[P], const double (&sy)[P],
+                                                  const double (&sz)[P], float (&Q)[P]) {
+  float Kr[S - 1][P], Ki[S - 1][P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) Q[q] = 0.f;
+#pragma unroll
+  for (int b = 0; b < S; ++b) {
+    const double4 Ub = U[b];
+    float Fr[P], Fi[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      float c, s;
+      sat_exp(Ub, sx[q], sy[q], sz[q], c, s);
+      Fr[q] = c;
+      Fi[q] = -s;
+      if (MODE != kOpen) {
+        float m = ((hid >> b) & 1u) ? 0.f : 1.f;
+        if (MODE == kMixed && ((mix >> b) & 1u)) m = visible_row(rows[b], sx[q], sy[q], sz[q]) ? m : 0.f;
+        Fr[q] *= m;
+        Fi[q] *= m;
+      }
+    }
+    if (b > 0) {
+      float Hr[P], Hi[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) Hr[q] = Hi[q] = 0.f;
+      const float4 *col = reinterpret_cast<const float4 *>(cf + form_col0(b));
+#pragma unroll
+      for (int a2 = 0; a2 < b; a2 += 2) {
+        const float4 c2 = col[a2 / 2];  // coefficients of pairs (a2, b) and (a2 + 1, b)
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          Hr[q] = fmaf(c2.x, Kr[a2][q], fmaf(-c2.y, Ki[a2][q], Hr[q]));
+          Hi[q] = fmaf(c2.x, Ki[a2][q], fmaf(c2.y, Kr[a2][q], Hi[q]));
+        }
+        if (a2 + 1 < b) {
+#pragma unroll
+          for (int q = 0; q < P; ++q) {
+            Hr[q] = fmaf(c2.z, Kr[a2 + 1][q], fmaf(-c2.w, Ki[a2 + 1][q], Hr[q]));
+            Hi[q] = fmaf(c2.z, Ki[a2 + 1][q], fmaf(c2.w, Kr[a2 + 1][q], Hi[q]));
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < P; ++q) Q[q] = fmaf(Hr[q], Fr[q], fmaf(-Hi[q], Fi[q], Q[q]));
+    }
+    if (b < S - 1) {
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        Kr[b][q] = Fr[q];
+        Ki[b][q] = -Fi[q];
+      }
+    }
+  }
+}
+
 template <int S>
-__global__ void __launch_bounds__(kFormNT, 1) k_form_adjoint(const FormParams p) {
-  constexpr int B = form_pairs(S);
+__global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams p) {
   constexpr int CB = form_coef_stride(S);
-  constexpr int NW = kFormNT / 32;
+  constexpr int NW = kFormAdjNT / 32;
   constexpr int ST = 3;
   constexpr int P = kFormAdjP;
   __shared__ __align__(128) FormAdjStage<S> s_stage[ST];
@@ -307,7 +378,6 @@ __global__ void __launch_bounds__(kFormNT, 1) k_form_adjoint(const FormParams p)
 #pragma unroll
   for (int q = 0; q < P; ++q) ks[q] = kc[q] = 0.f;
   const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
-  const float4 pass32 = make_float4(0.f, 0.f, 0.f, -4.f);
   unsigned long long evaluated = 0;
   int next = 0;
   for (int it = 0; it < ntile; ++it) {
@@ -338,55 +408,20 @@ __global__ void __launch_bounds__(kFormNT, 1) k_form_adjoint(const FormParams p)
       const unsigned mix = __ballot_sync(0xffffffffu, lane <= S && st == 1);
       const bool snap_hidden = __ballot_sync(0xffffffffu, lane == S && st == 0) != 0;
       if (!tile_ok || snap_hidden || S - __popc(hid) < 2) continue;
-      evaluated += static_cast<unsigned long long>(32 * P) * B;
-      const double4 *U = g.U + k * S;
-      const float2 *cf = g.coef + k * CB;
-      float Kr[S - 1][P], Ki[S - 1][P], Q[P];
+      evaluated += static_cast<unsigned long long>(32 * P) * form_pairs(S);
+      float Q[P];
+      // two code paths only: a third (hidden satellites without mixed rows)
+      // measured slower, the unrolled bodies competing for instruction cache
+      if (mix | hid) {
+        form_adj_snapshot<S, P, kMixed>(g.U + k * S, g.coef + k * CB, g.rows + k * S, hid, mix, sx, sy, sz, Q);
+        if ((mix >> S) & 1u) {
+          const double4 re = p.snap_rows ? g.snap[k] : pass;
 #pragma unroll
-      for (int q = 0; q < P; ++q) Q[q] = 0.f;
-#pragma unroll
-      for (int b = 0; b < S; ++b) {
-        const double4 Ub = U[b];
-        const double4 rb = (mix >> b) & 1u ? g.rows[k * S + b] : pass;
-        float Fr[P], Fi[P];
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-          float c, s;
-          sat_exp(Ub, sx[q], sy[q], sz[q], c, s);
-          float m = ((hid >> b) & 1u) ? 0.f : 1.f;
-          if ((mix >> b) & 1u) m = visible_row(rb, sx[q], sy[q], sz[q]) ? m : 0.f;
-          Fr[q] = m * c;
-          Fi[q] = -m * s;
+          for (int q = 0; q < P; ++q)
+            if (!visible_row(re, sx[q], sy[q], sz[q])) Q[q] = 0.f;
         }
-        if (b > 0) {
-          float Hr[P], Hi[P];
-#pragma unroll
-          for (int q = 0; q < P; ++q) Hr[q] = Hi[q] = 0.f;
-#pragma unroll
-          for (int a = 0; a < b; ++a) {
-            const float2 c = cf[pair_index<S>(a, b)];
-#pragma unroll
-            for (int q = 0; q < P; ++q) {
-              Hr[q] = fmaf(c.x, Kr[a][q], fmaf(-c.y, Ki[a][q], Hr[q]));
-              Hi[q] = fmaf(c.x, Ki[a][q], fmaf(c.y, Kr[a][q], Hi[q]));
-            }
-          }
-#pragma unroll
-          for (int q = 0; q < P; ++q) Q[q] = fmaf(Hr[q], Fr[q], fmaf(-Hi[q], Fi[q], Q[q]));
-        }
-        if (b < S - 1) {
-#pragma unroll
-          for (int q = 0; q < P; ++q) {
-            Kr[b][q] = Fr[q];
-            Ki[b][q] = -Fi[q];
-          }
-        }
-      }
-      if ((mix >> S) & 1u) {
-        const double4 re = p.snap_rows ? g.snap[k] : pass;
-#pragma unroll
-        for (int q = 0; q < P; ++q)
-          if (!visible_row(re, sx[q], sy[q], sz[q])) Q[q] = 0.f;
+      } else {
+        form_adj_snapshot<S, P, kOpen>(g.U + k * S, g.coef + k * CB, g.rows + k * S, hid, mix, sx, sy, sz, Q);
       }
 #pragma unroll
       for (int q = 0; q < P; ++q) acc[q] += Q[q];
@@ -404,13 +439,13 @@ __global__ void __launch_bounds__(kFormNT, 1) k_form_adjoint(const FormParams p)
     out[wpix + 32 * q + lane] = static_cast<double>(ks[q]) - static_cast<double>(kc[q]);
 }
 
-int form_adjoint_pixels_per_block() { return (kFormNT / 32) * 32 * kFormAdjP; }
+int form_adjoint_pixels_per_block() { return (kFormAdjNT / 32) * 32 * kFormAdjP; }
 
 template <int S>
 static cudaError_t form_fwd_inst(const FormParams &p, int nchunk, cudaStream_t st) {
-  const long long gx = (p.T + kFormNT / 32 - 1) / (kFormNT / 32);
+  const long long gx = (p.T + kFormFwdNT / 32 - 1) / (kFormFwdNT / 32);
   if (gx > 0x7fffffffLL || nchunk > 65535) return cudaErrorInvalidValue;
-  k_form_forward<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormNT, 0, st>>>(p);
+  k_form_forward<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormFwdNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -418,7 +453,7 @@ template <int S>
 static cudaError_t form_adj_inst(const FormParams &p, int nchunk, cudaStream_t st) {
   const long long gx = (p.Jpad + form_adjoint_pixels_per_block() - 1) / form_adjoint_pixels_per_block();
   if (nchunk > 65535) return cudaErrorInvalidValue;
-  k_form_adjoint<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormNT, 0, st>>>(p);
+  k_form_adjoint<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormAdjNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -464,23 +499,28 @@ __global__ void k_form_bound(long long n, const double *U, long long m, const do
   if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(b)));
 }
 
-// c'[t][b] = c[t B + b] e^{+2 pi i off} (FP64 rotation), zero in the padding.
-__global__ void k_form_stage_coef(long long T, int B, int CB, const float2 *coef, const double *off,
+// c'[t][form_col0(b) + a] = c[t B + pair(a, b)] e^{+2 pi i off} (FP64
+// rotation), zero in the padding of each column.
+__global__ void k_form_stage_coef(long long T, int S, int CB, const float2 *coef, const double *off,
                                   float2 *out) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= T * CB) return;
   const long long t = i / CB;
-  const int b = static_cast<int>(i - t * CB);
-  if (b >= B) {
+  const int r = static_cast<int>(i - t * CB);
+  int b = 1;
+  while (b + 1 < S && form_col0(b + 1) <= r) ++b;
+  const int a = r - form_col0(b);
+  if (a >= b) {
     out[i] = make_float2(0.f, 0.f);
     return;
   }
-  const float2 c = coef[t * B + b];
+  const long long k = t * form_pairs(S) + (a * S - a * (a + 1) / 2 + (b - a - 1));
+  const float2 c = coef[k];
   if (!off) {
     out[i] = c;
     return;
   }
-  const double o = off[t * B + b];
+  const double o = off[k];
   double sn, cs;
   sincospi(2.0 * (o - rint(o)), &sn, &cs);
   const double re = c.x, im = c.y;
@@ -529,7 +569,7 @@ cudaError_t launch_form_stage(long long T, int S, const double *U, const double 
 cudaError_t launch_form_stage_coef(long long T, int S, const float2 *coef, const double *off,
                                    float2 *out, cudaStream_t st) {
   const int CB = form_coef_stride(S);
-  k_form_stage_coef<<<nblk(T * CB, 256), 256, 0, st>>>(T, form_pairs(S), CB, coef, off, out);
+  k_form_stage_coef<<<nblk(T * CB, 256), 256, 0, st>>>(T, S, CB, coef, off, out);
   return cudaGetLastError();
 }
 

@@ -54,11 +54,18 @@ struct AdjParams {
 // Satellite-formation mode (formation.cu): every sample is a pair a < b of the
 // S satellites of one snapshot (lexicographic pair order, samples t-major),
 // u = U[t][a] - U[t][b].
-constexpr int kFormNT = 256;       // threads per block (both kernels)
+constexpr int kFormFwdNT = 256;    // forward: threads per block (one snapshot per warp)
+constexpr int kFormAdjNT = 256;    // adjoint: threads per block
 constexpr int kFormSnapTile = 8;   // snapshots per adjoint staging tile
 constexpr int kFormFoldTiles = 32; // forward: pixel tiles between FP64 folds
 __host__ __device__ constexpr int form_pairs(int S) { return S * (S - 1) / 2; }
-__host__ __device__ constexpr int form_coef_stride(int S) { return (form_pairs(S) + 1) & ~1; }
+// Adjoint coefficient layout per snapshot: column b (pairs a < b, a = 0..b-1)
+// starts at form_col0(b) and is padded to an even length with zeros, so that
+// two coefficients load as one 16-byte shared-memory read.
+// Columns 1..b-1 hold b' entries each, rounded up to even:
+// sum = b(b-1)/2 + (odd b' in [1, b)) = b(b-1)/2 + floor(b/2).
+__host__ __device__ constexpr int form_col0(int b) { return b * (b - 1) / 2 + b / 2; }
+__host__ __device__ constexpr int form_coef_stride(int S) { return form_col0(S); }
 
 struct FormParams {
   const double4 *U;       // [T][S] satellite vectors in wavelengths (.w unused)
@@ -73,7 +80,8 @@ struct FormParams {
   int tiles_per_chunk;    // forward
   int snaps_per_chunk;    // adjoint, a multiple of kFormSnapTile
   int nchunk;
-  const float2 *coef;     // adjoint: [T][form_coef_stride(S)] coefficients, offsets applied
+  const float2 *coef;     // adjoint: [T][form_coef_stride(S)] coefficients, offsets applied,
+                          // column layout of form_col0
   double2 *part_fwd;      // [chunk][T * B]
   double *part_adj;       // [chunk][Jpad]
   unsigned long long *counter;
