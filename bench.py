@@ -9,6 +9,12 @@ adjoint pass, split precision.  Terms per step = 2 x 388,800 x 786,432.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Beside the headline, the line carries "formation_mode": the same step through
+the formation entry points (viss_plan_set_formation: the samples given as the
+satellites' vectors, S exponentials per pixel and snapshot instead of one per
+sample), with its own roofline (FP32 FMA issue) and its rel-L2 against the
+direct kernels.  --formation makes that the whole run.
+
 N > 1 runs under torchrun: every rank is an independent replica (its own
 observation day, no data-path collective; weak scaling), timed on the device
 and reduced as the max over ranks.  --impl reference times the FP64 CPU
@@ -827,6 +833,8 @@ def main():
                     help="benchmark configuration (default: the headline one)")
     ap.add_argument("--formation", action="store_true",
                     help="run the step through the formation entry points (satellite vectors)")
+    ap.add_argument("--no-formation-compare", dest="formation_compare", action="store_false",
+                    help="skip timing the formation entry points beside the headline step")
     ap.add_argument("--stream-days", type=int, default=4,
                     help="days of the stream workload")
     args = ap.parse_args()
@@ -858,6 +866,15 @@ def main():
             print(json.dumps(run_stream(args)), flush=True)
             return
         res = run_ours(args, rank, world, local_rank)
+        if not args.formation and args.formation_compare and args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz", "c3_small"):
+            # the same step through the formation entry points (satellite vectors
+            # instead of per-sample uvw), reported beside the headline
+            f = run_formation(args, rank, world, local_rank)
+            if res is not None and f is not None:
+                res["formation_mode"] = {k: f[k] for k in ("value", "unit", "ms_per_step", "e2e", "roofline",
+                                                           "kernel_ms", "forward_rel_l2_vs_direct", "clocks")}
+                res["formation_mode"]["entry_points"] = ("viss_plan_set_formation, viss_forward_formation, "
+                                                         "viss_adjoint_formation")
         if res is not None:
             print(json.dumps(res), flush=True)
     finally:

@@ -169,7 +169,7 @@ int viss_plan_set_channels(viss_plan *plan, int channels);
  *   off      T x S(S-1)/2 phase offsets in turns, or NULL
  *   occ_sat  T x S x 4 occulter rows of the satellites (Moon), or NULL
  *   occ_snap T x 4 rows of the snapshots (Earth cap), or NULL
- * S must be 4, 6, 8 or 10.  Synchronises `stream` once.  No counterpart in the
+ * 2 <= S <= 10.  Synchronises `stream` once.  No counterpart in the
  * reference. */
 int viss_plan_set_formation(viss_plan *plan, int64_t T, int S, const double *U, const double *off,
                             const double *occ_sat, const double *occ_snap, void *stream);

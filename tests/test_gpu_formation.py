@@ -35,6 +35,11 @@ def _case(cfg, f, dev, seed_off=None):
     ("c2", 1e7, 8, 16, 30, False),
     ("c3_10mhz", 1e7, 10, 16, 24, True),
     ("c3_1mhz", 1e6, 10, 32, 16, False),
+    ("c1", 1e6, 4, 16, 200, True),        # no occultation; several adjoint chunks
+    ("c2", 1e7, 6, 16, 130, False),       # Moon only, T not a multiple of 8
+    ("c3_10mhz", 1e7, 5, 16, 40, False),  # odd S
+    ("c3_10mhz", 1e7, 7, 16, 19, True),
+    ("c3_10mhz", 1e7, 2, 16, 64, False),
 ])
 def test_formation_matches_direct_and_oracle(oracle, cuda_device, cfgname, f, S, nside, T, with_off):
     cfg = synth.scaled(synth.CONFIGS[cfgname], nside=nside, n_snap=T, n_sat=S)
@@ -71,7 +76,7 @@ def test_formation_rejects_invalid_use(cuda_device):
         plan.form_T, plan.form_B = 1, 1
         plan.forward_formation(torch.ones(lmn.shape[0], device=cuda_device))
     with pytest.raises(VissError, match="S must be"):
-        plan.set_formation(torch.zeros((3, 7, 3), dtype=torch.float64))
+        plan.set_formation(torch.zeros((3, 11, 3), dtype=torch.float64))
     plan.set_formation(torch.zeros((3, 4, 3), dtype=torch.float64))
     V = torch.empty(18, dtype=torch.complex64, device=cuda_device)
     sky = torch.ones(lmn.shape[0], device=cuda_device)
@@ -81,3 +86,27 @@ def test_formation_rejects_invalid_use(cuda_device):
     U[1, 2, 0] = float("nan")
     with pytest.raises(VissError, match="non-finite"):
         plan.set_formation(U)
+
+
+def test_formation_hidden_snapshots(oracle, cuda_device):
+    """A snapshot row that hides the whole sky (thr > 1) zeroes that snapshot's
+    samples exactly; a satellite row that hides everything zeroes its pairs."""
+    cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], nside=16, n_snap=12, n_sat=6)
+    obs = synth.make_observation(cfg)
+    g = pipeline.upload(obs, 1e7, device=cuda_device)
+    U, occ_sat, occ_snap = pipeline.formation_inputs(obs, 1e7, device=cuda_device, occ=g.occ)
+    occ_snap = occ_snap.clone()
+    occ_snap[3] = torch.tensor([0.0, 0.0, 1.0, 2.0], dtype=torch.float64)
+    occ_sat = occ_sat.clone()
+    occ_sat[5, 2] = torch.tensor([0.0, 0.0, 1.0, 2.0], dtype=torch.float64)
+    g.plan.set_formation(U, None, occ_sat, occ_snap)
+    B = 15
+    V = g.plan.forward_formation(g.sky).cpu().numpy().reshape(12, B)
+    assert np.all(V[3] == 0)
+    pairs_with_2 = [k for k, (a, b) in enumerate(synth.baseline_pairs(6)) if 2 in (a, b)]
+    assert np.all(V[5, pairs_with_2] == 0)
+    # the rest against the oracle on the same rows
+    occ = torch.cat([occ_sat.reshape(-1, 4), occ_snap]).cpu().numpy()
+    Vo = oracle.forward(g.uvw.cpu().numpy(), g.lmn.cpu().numpy(), g.sky.cpu().numpy().astype(np.float64),
+                        obs.refs, occ).reshape(12, B)
+    assert rel_l2(V, Vo) <= 1e-5, rel_l2(V, Vo)

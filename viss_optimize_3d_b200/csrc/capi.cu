@@ -591,8 +591,8 @@ int viss_plan_set_channels(viss_plan *p, int channels) {
 int viss_plan_set_formation(viss_plan *p, int64_t T, int S, const double *U, const double *off,
                             const double *occ_sat, const double *occ_snap, void *stream) {
   if (!p || T < 1 || !U) return fail(VISS_ERR_ARG, "viss_plan_set_formation: bad arguments");
-  if (S != 4 && S != 6 && S != 8 && S != 10)
-    return fail(VISS_ERR_ARG, "viss_plan_set_formation: S must be 4, 6, 8 or 10 satellites");
+  if (S < 2 || S > 10)
+    return fail(VISS_ERR_ARG, "viss_plan_set_formation: S must be 2 to 10 satellites");
   const long long B = viss::form_pairs(S);
   if (T * B >= (1LL << 31)) return fail(VISS_ERR_ARG, "viss_plan_set_formation: too many samples");
   const cudaStream_t st = as_stream(stream);

@@ -460,9 +460,14 @@ static cudaError_t form_adj_inst(const FormParams &p, int nchunk, cudaStream_t s
 cudaError_t launch_form_forward(const FormParams &p, int S, int nchunk, cudaStream_t st) {
   if (p.T <= 0 || p.ntiles <= 0) return cudaSuccess;
   switch (S) {
+    case 2: return form_fwd_inst<2>(p, nchunk, st);
+    case 3: return form_fwd_inst<3>(p, nchunk, st);
     case 4: return form_fwd_inst<4>(p, nchunk, st);
+    case 5: return form_fwd_inst<5>(p, nchunk, st);
     case 6: return form_fwd_inst<6>(p, nchunk, st);
+    case 7: return form_fwd_inst<7>(p, nchunk, st);
     case 8: return form_fwd_inst<8>(p, nchunk, st);
+    case 9: return form_fwd_inst<9>(p, nchunk, st);
     case 10: return form_fwd_inst<10>(p, nchunk, st);
     default: return cudaErrorInvalidValue;
   }
@@ -471,9 +476,14 @@ cudaError_t launch_form_forward(const FormParams &p, int S, int nchunk, cudaStre
 cudaError_t launch_form_adjoint(const FormParams &p, int S, int nchunk, cudaStream_t st) {
   if (p.T <= 0 || p.Jpad <= 0) return cudaSuccess;
   switch (S) {
+    case 2: return form_adj_inst<2>(p, nchunk, st);
+    case 3: return form_adj_inst<3>(p, nchunk, st);
     case 4: return form_adj_inst<4>(p, nchunk, st);
+    case 5: return form_adj_inst<5>(p, nchunk, st);
     case 6: return form_adj_inst<6>(p, nchunk, st);
+    case 7: return form_adj_inst<7>(p, nchunk, st);
     case 8: return form_adj_inst<8>(p, nchunk, st);
+    case 9: return form_adj_inst<9>(p, nchunk, st);
     case 10: return form_adj_inst<10>(p, nchunk, st);
     default: return cudaErrorInvalidValue;
   }
