@@ -63,6 +63,8 @@ MUFU_TERMS_PER_CLK_PER_SM = 8     # 16 MUFU results/clk/SM, sin + cos per term
 # profiles/dram_c3_10mhz.md; bench.py cannot read DRAM counters itself.
 NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 56217088 + 45796096, "k_adjoint": 60853248 + 45885696}}
 NCU_TRAFFIC_SOURCE = "profiles/dram_c3_10mhz.md (ncu, one pass, full-size workload)"
+FORM_NCU_TRAFFIC = {"c3_10mhz": {"k_form_forward": 32984064 + 449792, "k_form_adjoint": 36857344 + 32256}}
+FORM_NCU_TRAFFIC_SOURCE = "profiles/launches_bench_formation_c3_10mhz.md (ncu, one pass, full-size workload)"
 
 
 def peaks():
@@ -487,7 +489,10 @@ def run_formation(args, rank, world, local_rank):
                      "unit": "Gterms/s", "frac": round(achieved / peak_terms, 4),
                      "peak_source": f"128 FP32 lanes/clk/SM / {FORM_FFMA_PER_TERM} FFMA per term x {nsm} SMs "
                                     f"x sm_max_mhz ({pk_kind})",
-                     "evaluated_frac": round(dom_eval / (K * J), 4), "traffic": None},
+                     "evaluated_frac": round(dom_eval / (K * J), 4),
+                     "traffic": FORM_NCU_TRAFFIC.get(args.workload, {}).get(f"k_form_{dom}"),
+                     "traffic_unit": "bytes per launch",
+                     "traffic_source": FORM_NCU_TRAFFIC_SOURCE if args.workload in FORM_NCU_TRAFFIC else None},
         "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
         "forward_rel_l2_vs_direct": float(f"{rel_v:.3e}"),
         "gpu_launches": 10 * args.steps,
