@@ -599,7 +599,7 @@ def run_reconstruction(args):
 
     dev = torch.device("cuda", 0)
     cfg = synth.CONFIGS["c5"]
-    p = reconstruct.make_problem(cfg, device=dev, seed=0)
+    p = reconstruct.make_problem(cfg, device=dev, seed=0, formation=args.formation)
     p64 = reconstruct.make_problem(cfg, device=dev, seed=0, fp64=True)
     stream = torch.cuda.current_stream(dev)
     K, J = cfg.n_samples, cfg.npix
@@ -638,8 +638,10 @@ def run_reconstruction(args):
         "steps": 1, "warmup": 2, "ms_per_step": round(t_eval * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64-phase/f32-sincos",
         "data": "synthetic (seeded, see synth.py)",
-        "config": {"workload": WORKLOAD_TEXT["c5"], "pixels": J, "samples": K,
-                   "terms_per_evaluation": terms_eval},
+        "config": {"workload": WORKLOAD_TEXT["c5"] + ("; formation mode" if args.formation else ""),
+                   "pixels": J, "samples": K, "terms_per_evaluation": terms_eval,
+                   "operator": "FormationModel (viss_*_formation)" if args.formation
+                               else "VisibilityModel (viss_forward / viss_adjoint)"},
         "gradient": {"sky_rel_err_split_vs_fp64": float(f"{float((gx - gx64).norm() / gx64.norm()):.3e}"),
                      "positions_rel_err_split_vs_fp64": float(f"{float((gd - gd64).norm() / gd64.norm()):.3e}")},
         "lbfgs": {"iterations": 200, "evaluations": len(hist), "seconds": round(t_lbfgs, 2),

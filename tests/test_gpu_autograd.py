@@ -77,3 +77,26 @@ def test_lbfgs_beats_dirty_image(small):
     # satellite leaves the baselines unchanged, so compare centred offsets)
     c = lambda t: t - t.mean(dim=0, keepdim=True)
     assert float((c(delta) - c(p.delta_true)).norm()) < 0.5 * float(c(p.delta_true).norm())
+
+
+def test_formation_operator_gradients(small, cuda_device):
+    """The formation operator (satellite vectors in, autograd.FormationModel):
+    loss and gradients against the FP64 direct operator, within the split
+    path's own tolerances, and closer still to the split direct operator."""
+    p, p64 = small
+    pf = reconstruct.make_problem(p.cfg, device=cuda_device, seed=1, formation=True)
+    assert torch.equal(pf.V_obs, p.V_obs)
+    gen = torch.Generator(device="cpu").manual_seed(3)
+    x = (p.x_true.cpu() * (1 + 0.3 * torch.randn(p.x_true.shape, generator=gen))).to(p.x_true.device)
+    d = torch.randn(p.delta_true.shape, generator=gen, dtype=torch.float64).to(x.device) * 3.0
+    L64, gx64, gd64 = _grads(p64, x, d)
+    L32, gx32, gd32 = _grads(p, x, d)
+    Lf, gxf, gdf = _grads(pf, x, d)
+    assert abs(Lf - L64) < 1e-5 * L64
+    assert float((gxf - gx64).norm() / gx64.norm()) < 1e-4
+    assert float((gdf - gd64).norm() / gd64.norm()) < 1e-3
+    assert float((gxf - gx32).norm() / gx32.norm()) < 1e-4
+    dirty = reconstruct.dirty_image(pf)
+    xr, _dr, hist = reconstruct.reconstruct(pf, iters=40)
+    assert hist[-1] < 0.1 * hist[0]
+    assert reconstruct.rel_l2(xr, pf.x_true) < reconstruct.rel_l2(dirty, pf.x_true)

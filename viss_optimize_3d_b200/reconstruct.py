@@ -10,7 +10,10 @@ for the sky x (per-pixel intensity, Omega = 4 pi / npix) and a constant
 position offset delta per satellite (the 30 coordinates of 10 satellites),
 with u(delta) = (P_a + delta_a - P_b - delta_b) / lambda, using
 torch.optim.LBFGS on the GPU operator of autograd.py (exponentials recomputed
-in every pass, never stored).  w are the shell-histogram DCF weights.
+in every pass, never stored).  w are the shell-histogram DCF weights.  With
+formation=True the operator is FormationModel: the same A through the
+formation entry points, its input the satellite vectors
+U = (P0 + delta - c) / lambda (c: each snapshot's nominal centroid).
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ import numpy as np
 import torch
 
 from . import api, synth
-from .autograd import VisibilityModel
+from .autograd import FormationModel, VisibilityModel
 from .pipeline import build_occulters
 
 
@@ -37,7 +40,8 @@ class Problem:
     V_obs: torch.Tensor       # (K,) observed visibilities
     sigma: float
     w: torch.Tensor           # (K,) weights
-    model: VisibilityModel
+    model: VisibilityModel | FormationModel
+    centre: torch.Tensor | None = None  # (T, 1, 3) per-snapshot origin of U (formation model)
 
 
 def baselines(P0: torch.Tensor, delta: torch.Tensor, pairs: torch.Tensor, lam: float) -> torch.Tensor:
@@ -47,8 +51,13 @@ def baselines(P0: torch.Tensor, delta: torch.Tensor, pairs: torch.Tensor, lam: f
     return (d / lam).reshape(-1, 3)
 
 
+def formation_vectors(P0: torch.Tensor, delta: torch.Tensor, centre: torch.Tensor, lam: float) -> torch.Tensor:
+    """U (T, S, 3) in wavelengths: U_a - U_b is baselines()' u of pair (a, b)."""
+    return (P0 + delta[None, :, :] - centre) / lam
+
+
 def make_problem(cfg: synth.ObsConfig, device="cuda", seed: int = 0, snr: float = 20.0,
-                 pos_sigma_m: float = 5.0, fp64: bool = False) -> Problem:
+                 pos_sigma_m: float = 5.0, fp64: bool = False, formation: bool = False) -> Problem:
     obs = synth.make_observation(cfg)
     f = cfg.freqs_hz[0]
     lam = synth.C_LIGHT / f
@@ -72,11 +81,27 @@ def make_problem(cfg: synth.ObsConfig, device="cuda", seed: int = 0, snr: float 
     _dg, wt = api.weights(torch.as_tensor(w_np, dtype=torch.float32, device=device), bll, gs, dcf,
                           obs.nr(f))
     w = wt / wt.mean()
-    return Problem(cfg, lam, omega, P0, pairs, delta_true, x_true, V_obs, sigma, w, model)
+    centre = None
+    if formation:
+        if fp64:
+            raise ValueError("the formation entry points are split precision only")
+        T, S = cfg.n_snap, cfg.n_sat
+        occ_sat = occ[:T * S].reshape(T, S, 4) if cfg.moon else None
+        occ_snap = occ[T * S:T * S + T] if obs.earth_rows is not None else None
+        model = FormationModel(lmn, occ_sat, occ_snap)
+        centre = P0.mean(dim=1, keepdim=True)
+    return Problem(cfg, lam, omega, P0, pairs, delta_true, x_true, V_obs, sigma, w, model, centre)
+
+
+def operator_input(p: Problem, delta: torch.Tensor) -> torch.Tensor:
+    """What the problem's model takes: u (K, 3) or, for the formation model, U (T, S, 3)."""
+    if p.centre is not None:
+        return formation_vectors(p.P0, delta, p.centre, p.lam)
+    return baselines(p.P0, delta, p.pairs, p.lam)
 
 
 def loss(p: Problem, x: torch.Tensor, delta: torch.Tensor) -> torch.Tensor:
-    V = p.model(x * p.omega, baselines(p.P0, delta, p.pairs, p.lam))
+    V = p.model(x * p.omega, operator_input(p, delta))
     r = (V - p.V_obs).to(torch.complex128) * p.w.to(torch.float64)
     return (r.real.square() + r.imag.square()).sum() / (p.sigma ** 2)
 
@@ -86,7 +111,7 @@ def dirty_image(p: Problem) -> torch.Tensor:
     nominal positions, scaled by the least-squares factor onto the true sky
     (the dirty image has arbitrary units)."""
     with torch.no_grad():
-        u0 = baselines(p.P0, torch.zeros_like(p.delta_true), p.pairs, p.lam)
+        u0 = operator_input(p, torch.zeros_like(p.delta_true))
         img = p.model.adjoint_raw((p.V_obs * p.w).contiguous(), u0).to(torch.float64)
         t = p.x_true.to(torch.float64)
         a = float((img * t).sum() / (img * img).sum())
