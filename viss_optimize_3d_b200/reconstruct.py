@@ -138,7 +138,7 @@ def reconstruct(p: Problem, iters: int = 200, positions: bool = True, x0=None,
         opt.zero_grad()
         L = loss(p, x, delta)
         L.backward()
-        hist.append(float(L))
+        hist.append(float(L.detach()))
         return L
 
     opt.step(closure)
