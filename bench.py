@@ -572,6 +572,37 @@ def run_batched(args):
     t_single_graph = timed(g2.replay, max(1, args.steps // 2), 1)
     ok = all(torch.allclose(out_I[c], outs[c][1], rtol=1e-4, atol=1e-5 * outs[c][1].abs().max().item())
              for c in range(C))
+    del singles, outs
+    form = None
+    if args.formation_compare or args.formation:
+        # the same channels through the formation entry points: U (C, T, S, 3),
+        # one launch per kernel for all channels, graph replay
+        U = torch.stack([pipeline.formation_inputs(obs, f, device=dev, occ=occ)[0] for f in cfg.freqs_hz])
+        _u, occ_sat, occ_snap = pipeline.formation_inputs(obs, cfg.freqs_hz[0], device=dev, occ=occ)
+        fplan = api.Plan(lmn)
+        fplan.set_formation(U, None, occ_sat, occ_snap)
+        fV = torch.empty(C * K, dtype=torch.complex64, device=dev)
+        fI = torch.empty((C, J), dtype=torch.float32, device=dev)
+
+        def step_formation():
+            fplan.forward_formation(sky, out=fV)
+            fplan.adjoint_formation(coef, out=fI)
+
+        t_fstream = timed(step_formation, args.steps, args.warmup)
+        fg = torch.cuda.CUDAGraph()
+        step_formation()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(fg):
+            step_formation()
+        t_fgraph = timed(fg.replay, args.steps, 1)
+        rel_V = float(torch.linalg.norm((fV - out_V).to(torch.complex128)) / torch.linalg.norm(out_V.to(torch.complex128)))
+        rel_I = float(torch.linalg.norm((fI - out_I).double()) / torch.linalg.norm(out_I.double()))
+        form = {"value": round(terms / t_fgraph / 1e9, 3), "unit": UNIT, "graph_ms": round(t_fgraph * 1e3, 2),
+                "stream_ms": round(t_fstream * 1e3, 2), "launches_per_step": 2,
+                "V_rel_l2_vs_direct": float(f"{rel_V:.3e}"), "image_rel_l2_vs_direct": float(f"{rel_I:.3e}"),
+                "entry_points": "viss_plan_set_formation (U: C x T x S x 3), viss_plan_set_formation_channels, "
+                                "viss_forward_formation, viss_adjoint_formation"}
+        del fg
     res = {
         "metric": METRIC, "value": round(terms / t_graph / 1e9, 3), "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_graph * 1e3, 2),
@@ -586,6 +617,8 @@ def run_batched(args):
         "speedup_batched_graph_vs_per_channel": round(t_single / t_graph, 3),
         "images_agree": bool(ok),
     }
+    if form is not None:
+        res["formation_mode"] = form
     del graph, g2
     return res
 

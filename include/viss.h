@@ -173,10 +173,17 @@ int viss_plan_set_channels(viss_plan *plan, int channels);
  * reference. */
 int viss_plan_set_formation(viss_plan *plan, int64_t T, int S, const double *U, const double *off,
                             const double *occ_sat, const double *occ_snap, void *stream);
-/* V (T x S(S-1)/2 complex64) for sky (J FP32); flags VISS_NO_MASK, VISS_ACCUMULATE. */
+/* Frequency channels of a formation: the T snapshots given to
+ * viss_plan_set_formation are C channels of T / C snapshots each (channel-major;
+ * U scaled by each channel's wavelength, the occulter rows repeated per channel).
+ * Each channel has its own sky and image; one launch per kernel covers all.
+ * Reset to 1 by viss_plan_set_formation. */
+int viss_plan_set_formation_channels(viss_plan *plan, int channels);
+/* V (T x S(S-1)/2 complex64) for sky (C x J FP32); flags VISS_NO_MASK, VISS_ACCUMULATE. */
 int viss_forward_formation(viss_plan *plan, const float *sky, float *V, int flags, void *stream);
-/* image (J FP32) = scale * the adjoint of the formation's samples for coef
- * (T x S(S-1)/2 complex64); flags VISS_NO_MASK, VISS_ACCUMULATE. */
+/* image (C x J FP32) = scale * the adjoint of the formation's samples for coef
+ * (T x S(S-1)/2 complex64), each channel's samples into its own image;
+ * flags VISS_NO_MASK, VISS_ACCUMULATE. */
 int viss_adjoint_formation(viss_plan *plan, const float *coef, float *image, float scale, int flags,
                            void *stream);
 

@@ -110,3 +110,41 @@ def test_formation_hidden_snapshots(oracle, cuda_device):
     Vo = oracle.forward(g.uvw.cpu().numpy(), g.lmn.cpu().numpy(), g.sky.cpu().numpy().astype(np.float64),
                         obs.refs, occ).reshape(12, B)
     assert rel_l2(V, Vo) <= 1e-5, rel_l2(V, Vo)
+
+
+def test_formation_channels(oracle, cuda_device):
+    """Frequency channels in one launch per kernel (set_formation with
+    U (C, T, S, 3)): every channel's V and image against the oracle on that
+    channel's uvw and sky; the occulter rows are shared."""
+    cfg = synth.scaled(synth.CONFIGS["c4"], nside=16, n_snap=24, freqs_hz=(1e6, 4.5e6, 1e7))
+    obs = synth.make_observation(cfg)
+    C, K, J = 3, cfg.n_samples, cfg.npix
+    g = pipeline.upload(obs, cfg.freqs_hz[0], device=cuda_device)
+    Us, skies = [], []
+    for f in cfg.freqs_hz:
+        U, occ_sat, occ_snap = pipeline.formation_inputs(obs, f, device=cuda_device, occ=g.occ)
+        Us.append(U)
+        skies.append(torch.as_tensor(obs.sky_at(f) * 4 * np.pi / J, dtype=torch.float32, device=cuda_device))
+    plan = g.plan
+    plan.set_formation(torch.stack(Us), None, occ_sat, occ_snap)
+    sky = torch.stack(skies)
+    V = plan.forward_formation(sky).cpu().numpy().reshape(C, K)
+    rng = np.random.default_rng(11)
+    a = (rng.standard_normal(C * K) + 1j * rng.standard_normal(C * K)).astype(np.complex64)
+    img = plan.adjoint_formation(torch.as_tensor(a, device=cuda_device), scale=2.0).cpu().numpy()
+    assert img.shape == (C, J)
+    lmn = g.lmn.cpu().numpy()
+    occ = g.occ.cpu().numpy()
+    for c, f in enumerate(cfg.freqs_hz):
+        uvw = obs.uvw(f)
+        Vo = oracle.forward(uvw, lmn, skies[c].cpu().numpy().astype(np.float64), obs.refs, occ)
+        assert rel_l2(V[c], Vo) <= 1e-5, (c, rel_l2(V[c], Vo))
+        Co = 2.0 * oracle.adjoint(uvw, a[c * K:(c + 1) * K].astype(np.complex128), lmn, obs.refs, occ)
+        assert rel_l2(img[c], Co) <= 1e-5, (c, rel_l2(img[c], Co))
+    # channels must divide the snapshots; set_formation resets to one channel
+    from viss_optimize_3d_b200._capi import VissError, check, lib
+    with pytest.raises(VissError, match="multiple of channels"):
+        check(lib.viss_plan_set_formation_channels(plan._h, 5), "set_formation_channels")
+    plan.set_formation(Us[0], None, occ_sat, occ_snap)
+    V0 = plan.forward_formation(skies[0]).cpu().numpy()
+    assert rel_l2(V0, V[0]) <= 1e-6

@@ -64,6 +64,7 @@ _SIGS = {
     "viss_plan_set_shapes": (_i, [_v, _i, _i]),
     "viss_plan_debug_drop_copy": (_i, [_v, _i]),
     "viss_plan_set_formation": (_i, [_v, _i64, _i, _v, _v, _v, _v, _v]),
+    "viss_plan_set_formation_channels": (_i, [_v, _i]),
     "viss_forward_formation": (_i, [_v, _v, _v, _i, _v]),
     "viss_adjoint_formation": (_i, [_v, _v, _v, _f, _i, _v]),
     "viss_plan_set_channels": (_i, [_v, _i]),

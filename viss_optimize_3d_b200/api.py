@@ -149,6 +149,8 @@ class Plan:
         self.K = 0
         self.channels = 1
         self.masked = False
+        self.form_T = self.form_S = self.form_B = 0   # formation mode (set_formation)
+        self.form_C = 1
         check(lib.viss_plan_set_pixels(self._h, self.J, _p(lmn), _stream(lmn)), "viss_plan_set_pixels")
         if uvw is not None:
             self.set_samples(uvw, off, refs, occ)
@@ -229,26 +231,47 @@ class Plan:
         (T, S, 3) FP64 satellite vectors in wavelengths; sample k = t * B + pair
         for the B = S(S-1)/2 pairs a < b in lexicographic order, u = U_a - U_b.
         off (T, B) turns, occ_sat (T, S, 4) and occ_snap (T, 4) occulter rows,
-        each optional.  Kept beside the plan's ordinary samples."""
+        each optional.  Kept beside the plan's ordinary samples.
+
+        U of shape (C, T, S, 3) gives C frequency channels of the same
+        snapshots (viss_plan_set_formation_channels): the occulter rows (T, ...)
+        are shared by the channels, off is (C, T, B); sky and image are then
+        C x J and V / coef C x T x B."""
         U = torch.as_tensor(U) if not isinstance(U, torch.Tensor) else U
+        C = 1
+        if U.dim() == 4:
+            C = int(U.shape[0])
+            U = U.reshape(-1, U.shape[2], U.shape[3])
         if U.dim() != 3 or U.shape[2] != 3:
-            raise ValueError("U must be (T, S, 3)")
+            raise ValueError("U must be (T, S, 3) or (C, T, S, 3)")
         T, S = int(U.shape[0]), int(U.shape[1])
         B = S * (S - 1) // 2
         U = _cuda(U.reshape(T * S, 3), torch.float64, self.device, shape_last=3)
         off = _cuda(None if off is None else torch.as_tensor(off).reshape(T * B), torch.float64, self.device)
-        occ_sat = _cuda(None if occ_sat is None else torch.as_tensor(occ_sat).reshape(T * S, 4),
-                        torch.float64, self.device, shape_last=4)
-        occ_snap = _cuda(occ_snap, torch.float64, self.device, shape_last=4)
+
+        def rows(r, width):
+            if r is None:
+                return None
+            r = torch.as_tensor(r).reshape(-1, 4)
+            if C > 1:
+                r = _cuda(r, torch.float64, self.device, shape_last=4).repeat(C, 1)
+            if r.shape[0] != T * width:
+                raise ValueError(f"occulter rows must cover {T // C} snapshots x {width}")
+            return _cuda(r, torch.float64, self.device, shape_last=4)
+
+        occ_sat, occ_snap = rows(occ_sat, S), rows(occ_snap, 1)
         check(lib.viss_plan_set_formation(self._h, T, S, _p(U), _p(off), _p(occ_sat), _p(occ_snap),
                                           _stream(U)), "viss_plan_set_formation")
-        self.form_T, self.form_S, self.form_B = T, S, B
+        self.form_T, self.form_S, self.form_B, self.form_C = T, S, B, C
+        if C > 1:
+            check(lib.viss_plan_set_formation_channels(self._h, C), "viss_plan_set_formation_channels")
 
     def forward_formation(self, sky, mask: bool = True, out: torch.Tensor | None = None):
-        """V (T * B complex64) of the formation's samples."""
+        """V (T * B complex64) of the formation's samples (channel-major with
+        channels: sky then holds C x J values)."""
         sky = _cuda(sky, torch.float32, self.device)
-        if sky.numel() != self.J:
-            raise ValueError(f"sky must hold {self.J} values")
+        if sky.numel() != self.form_C * self.J:
+            raise ValueError(f"sky must hold {self.form_C * self.J} values")
         n = self.form_T * self.form_B
         if out is None:
             out = torch.empty(n, dtype=torch.complex64, device=self.device)
@@ -261,16 +284,19 @@ class Plan:
 
     def adjoint_formation(self, coef, scale: float = 1.0, mask: bool = True,
                           out: torch.Tensor | None = None):
-        """img (J FP32) = scale * the adjoint of the formation's samples."""
+        """img (J FP32, or C x J with channels) = scale * the adjoint of the
+        formation's samples."""
         n = self.form_T * self.form_B
-        coef = _cuda(coef, torch.complex64, self.device)
+        nimg = self.form_C * self.J
+        coef = _cuda(coef, torch.complex64, self.device).reshape(-1)
         if coef.shape != (n,):
-            raise ValueError(f"coef must have shape ({n},)")
+            raise ValueError(f"coef must hold {n} values")
         if out is None:
-            out = torch.empty(self.J, dtype=torch.float32, device=self.device)
-        elif (out.dtype != torch.float32 or not out.is_contiguous() or out.numel() != self.J
+            out = torch.empty(nimg if self.form_C == 1 else (self.form_C, self.J), dtype=torch.float32,
+                              device=self.device)
+        elif (out.dtype != torch.float32 or not out.is_contiguous() or out.numel() != nimg
               or out.device != self.device):
-            raise ValueError(f"out must be a contiguous float32 tensor of {self.J} values on {self.device}")
+            raise ValueError(f"out must be a contiguous float32 tensor of {nimg} values on {self.device}")
         check(lib.viss_adjoint_formation(self._h, _p(coef), _p(out), float(scale),
                                          0 if mask else capi.VISS_NO_MASK, _stream(coef)),
               "viss_adjoint_formation")

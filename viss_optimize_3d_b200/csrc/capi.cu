@@ -135,8 +135,9 @@ struct viss_plan {
   float2 *coef = nullptr;  size_t coef_cap = 0;
   double max_turns = 0;
   // satellite-formation mode (viss_plan_set_formation)
-  long long form_T = 0;
+  long long form_T = 0;         // snapshots, all channels
   int form_S = 0;
+  int form_C = 1;               // channels (viss_plan_set_formation_channels)
   double4 *form_U = nullptr;    size_t form_U_cap = 0;
   double *form_off = nullptr;   size_t form_off_cap = 0;
   bool form_has_off = false;
@@ -631,9 +632,20 @@ int viss_plan_set_formation(viss_plan *p, int64_t T, int S, const double *U, con
     return fail(VISS_ERR_ARG, "viss_plan_set_formation: |U| or |off| exceeds 2^28 turns");
   p->form_T = T;
   p->form_S = S;
+  p->form_C = 1;
   p->form_has_off = off != nullptr;
   p->form_sat = occ_sat != nullptr;
   p->form_snap = occ_snap != nullptr;
+  return VISS_OK;
+}
+
+int viss_plan_set_formation_channels(viss_plan *p, int channels) {
+  if (!p || channels < 1) return fail(VISS_ERR_ARG, "viss_plan_set_formation_channels: bad arguments");
+  if (p->form_T <= 0) return fail(VISS_ERR_STATE, "viss_plan_set_formation_channels: formation not set");
+  if (p->form_T % channels != 0)
+    return fail(VISS_ERR_ARG, "viss_plan_set_formation_channels: the snapshot count is not a multiple of channels");
+  if (channels > 65535) return fail(VISS_ERR_ARG, "viss_plan_set_formation_channels: at most 65535 channels");
+  p->form_C = channels;
   return VISS_OK;
 }
 
@@ -658,6 +670,8 @@ static viss::FormParams form_params(viss_plan *p, int flags) {
   fp.ntiles = p->ntiles;
   fp.Jpad = p->Jpad;
   fp.T = p->form_T;
+  fp.channels = p->form_C;
+  fp.Tc = p->form_T / p->form_C;
   fp.counter = p->dev_words;
   fp.err = reinterpret_cast<int *>(p->dev_words + 1);
   return fp;
@@ -668,8 +682,11 @@ int viss_forward_formation(viss_plan *p, const float *sky, float *V, int flags, 
   const NvtxRange range("viss_forward_formation");
   const cudaStream_t st = as_stream(stream);
   const long long T = p->form_T, B = viss::form_pairs(p->form_S);
-  // about 16 waves of one block per SM, each block 8 snapshots x a chunk of tiles
-  const long long blocks = (T + viss::kFormFwdNT / 32 - 1) / (viss::kFormFwdNT / 32);
+  const int C = p->form_C;
+  const long long Tc = T / C;
+  // about 16 waves of one block per SM, each block 8 snapshots of one channel
+  // x a chunk of tiles
+  const long long blocks = C * ((Tc + viss::kFormFwdNT / 32 - 1) / (viss::kFormFwdNT / 32));
   long long c = (16LL * p->nsm + blocks - 1) / blocks;
   c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 4)));
   viss::FormParams fp = form_params(p, flags);
@@ -677,8 +694,9 @@ int viss_forward_formation(viss_plan *p, const float *sky, float *V, int flags, 
   const int nchunk = (p->ntiles + fp.tiles_per_chunk - 1) / fp.tiles_per_chunk;
   fp.nchunk = nchunk;
   if (int s = workspace(p, sizeof(double2) * static_cast<size_t>(nchunk) * T * B)) return s;
-  if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * p->Jpad, "pixel+sky records")) return s;
-  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, 1, st),
+  if (int s = ensure(p->pixsky, p->pixsky_cap, sizeof(double4) * p->Jpad * C, "pixel+sky records"))
+    return s;
+  VISS_CUDA(viss::launch_stage_sky(p->J, p->Jpad, p->pix, p->perm, sky, 1.0f, p->pixsky, C, st),
             "viss_forward_formation: sky");
   VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_forward_formation");
   fp.pix = p->pixsky;
@@ -704,15 +722,19 @@ int viss_adjoint_formation(viss_plan *p, const float *coef, float *image, float 
   VISS_CUDA(viss::launch_form_stage_coef(T, p->form_S, reinterpret_cast<const float2 *>(coef),
                                          p->form_has_off ? p->form_off : nullptr, p->form_coef, st),
             "viss_adjoint_formation: coefficients");
+  // chunks of each channel's snapshots: about 16 waves of CTAs in all, at
+  // least 4 staging tiles per chunk
+  const int C = p->form_C;
+  const long long Tc = T / C;
   const long long per = viss::form_adjoint_pixels_per_block();
-  const long long blocks = (p->Jpad + per - 1) / per;
+  const long long blocks = (p->Jpad + per - 1) / per * C;
   long long c = (16LL * p->nsm + blocks - 1) / blocks;
-  const long long max_c = std::max<long long>(1, (T + 4 * viss::kFormSnapTile - 1) / (4 * viss::kFormSnapTile));
-  c = std::max<long long>(1, std::min(c, std::min<long long>(max_c, 65535)));
-  long long spc = (T + c - 1) / c;
+  const long long max_c = std::max<long long>(1, (Tc + 4 * viss::kFormSnapTile - 1) / (4 * viss::kFormSnapTile));
+  c = std::max<long long>(1, std::min(c, std::min<long long>(max_c, 65535 / C)));
+  long long spc = (Tc + c - 1) / c;
   spc = (spc + viss::kFormSnapTile - 1) / viss::kFormSnapTile * viss::kFormSnapTile;
-  const int nchunk = static_cast<int>((T + spc - 1) / spc);
-  if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * p->Jpad)) return s;
+  const int nchunk = static_cast<int>((Tc + spc - 1) / spc);
+  if (int s = workspace(p, sizeof(double) * static_cast<size_t>(nchunk) * C * p->Jpad)) return s;
   VISS_CUDA(cudaMemsetAsync(p->dev_words, 0, 3 * sizeof(unsigned long long), st), "viss_adjoint_formation");
   viss::FormParams fp = form_params(p, flags);
   fp.pix = p->pix;
@@ -721,7 +743,7 @@ int viss_adjoint_formation(viss_plan *p, const float *coef, float *image, float 
   fp.coef = p->form_coef;
   fp.part_adj = static_cast<double *>(p->part);
   VISS_CUDA(viss::launch_form_adjoint(fp, p->form_S, nchunk, st), "viss_adjoint_formation: kernel");
-  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, 1, fp.part_adj, p->perm, scale, image,
+  VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, C, fp.part_adj, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_adjoint_formation: reduce");
   p->last_total = T * B * p->J;

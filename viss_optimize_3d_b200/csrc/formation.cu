@@ -140,8 +140,12 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
   volatile int *abort_flag = &s_abort;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long t = static_cast<long long>(blockIdx.x) * NW + warp;
-  const bool tok = t < p.T;
+  // a CTA never straddles channels: blockIdx.x = channel * blocks_per_channel + block
+  const long long bpc = (p.Tc + NW - 1) / NW;
+  const long long ch = blockIdx.x / bpc;
+  const long long tl = (blockIdx.x - ch * bpc) * NW + warp;
+  const bool tok = tl < p.Tc;
+  const long long t = ch * p.Tc + tl;
   const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
   if (lane < S) s_U[warp][lane] = tok ? p.U[t * S + lane] : make_double4(0, 0, 0, 0);
   if (lane <= S) {
@@ -158,7 +162,7 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
   const int t0 = blockIdx.y * p.tiles_per_chunk;
   const int ntile = max(0, min(t0 + p.tiles_per_chunk, p.ntiles) - t0);
   constexpr uint32_t kTileBytes = kTilePix * sizeof(double4);
-  const double4 *pix = p.pix;
+  const double4 *pix = p.pix + ch * p.Jpad;  // this channel's sky records
   auto issue = [&](int i, int stage) {
     mbar_expect_tx(&s_full[stage], kTileBytes);
     bulk_g2s(s_pix[stage], pix + static_cast<long long>(t0 + i) * kTilePix, kTileBytes,
@@ -341,8 +345,10 @@ __global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams
   // the warp's pixels lie in one kTilePix tile (32 P divides kTilePix)
   const float4 cone = tile_ok ? p.cones[wpix / kTilePix] : make_float4(0.f, 0.f, 1.f, 4.f);
 
-  const long long s0 = static_cast<long long>(blockIdx.y) * p.snaps_per_chunk;
-  const long long s1 = min(s0 + p.snaps_per_chunk, p.T);
+  // blockIdx.y = channel * nchunk + chunk; a chunk never leaves its channel
+  const long long ch = blockIdx.y / p.nchunk;
+  const long long s0 = ch * p.Tc + static_cast<long long>(blockIdx.y - ch * p.nchunk) * p.snaps_per_chunk;
+  const long long s1 = min(s0 + p.snaps_per_chunk, (ch + 1) * p.Tc);
   const int ntile = static_cast<int>((max(0LL, s1 - s0) + kFormSnapTile - 1) / kFormSnapTile);
   auto issue = [&](int i, int stage) {
     const long long ts = s0 + static_cast<long long>(i) * kFormSnapTile;
@@ -443,7 +449,7 @@ int form_adjoint_pixels_per_block() { return (kFormAdjNT / 32) * 32 * kFormAdjP;
 
 template <int S>
 static cudaError_t form_fwd_inst(const FormParams &p, int nchunk, cudaStream_t st) {
-  const long long gx = (p.T + kFormFwdNT / 32 - 1) / (kFormFwdNT / 32);
+  const long long gx = p.channels * ((p.Tc + kFormFwdNT / 32 - 1) / (kFormFwdNT / 32));
   if (gx > 0x7fffffffLL || nchunk > 65535) return cudaErrorInvalidValue;
   k_form_forward<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormFwdNT, 0, st>>>(p);
   return cudaGetLastError();
@@ -452,13 +458,15 @@ static cudaError_t form_fwd_inst(const FormParams &p, int nchunk, cudaStream_t s
 template <int S>
 static cudaError_t form_adj_inst(const FormParams &p, int nchunk, cudaStream_t st) {
   const long long gx = (p.Jpad + form_adjoint_pixels_per_block() - 1) / form_adjoint_pixels_per_block();
-  if (nchunk > 65535) return cudaErrorInvalidValue;
-  k_form_adjoint<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormAdjNT, 0, st>>>(p);
+  const long long gy = static_cast<long long>(p.channels) * nchunk;
+  if (gy > 65535) return cudaErrorInvalidValue;
+  k_form_adjoint<S><<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy)), kFormAdjNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_form_forward(const FormParams &p, int S, int nchunk, cudaStream_t st) {
   if (p.T <= 0 || p.ntiles <= 0) return cudaSuccess;
+  if (p.channels < 1 || p.Tc * p.channels != p.T) return cudaErrorInvalidValue;
   switch (S) {
     case 2: return form_fwd_inst<2>(p, nchunk, st);
     case 3: return form_fwd_inst<3>(p, nchunk, st);
@@ -475,6 +483,7 @@ cudaError_t launch_form_forward(const FormParams &p, int S, int nchunk, cudaStre
 
 cudaError_t launch_form_adjoint(const FormParams &p, int S, int nchunk, cudaStream_t st) {
   if (p.T <= 0 || p.Jpad <= 0) return cudaSuccess;
+  if (p.channels < 1 || p.Tc * p.channels != p.T) return cudaErrorInvalidValue;
   switch (S) {
     case 2: return form_adj_inst<2>(p, nchunk, st);
     case 3: return form_adj_inst<3>(p, nchunk, st);

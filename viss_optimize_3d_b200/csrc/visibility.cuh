@@ -72,18 +72,20 @@ struct FormParams {
   const double4 *occ;     // exact rows: [T*S] satellites, then [T] snapshots
   const float4 *occ32;    // the same, classification rows
   int sat_rows, snap_rows;  // 1 if those rows are present (and masking is on)
-  const double4 *pix;     // forward: pixel + sky records; adjoint: pixel records [Jpad]
+  const double4 *pix;     // forward: pixel + sky records [channel][Jpad]; adjoint: pixel records [Jpad]
   const float4 *cones;    // tile cones (cone_count layout)
   int ntiles;
   long long Jpad;
-  long long T;
+  long long T;            // snapshots, all channels (channel-major: t = channel * Tc + local)
+  long long Tc;           // snapshots per channel
+  int channels;
   int tiles_per_chunk;    // forward
   int snaps_per_chunk;    // adjoint, a multiple of kFormSnapTile
-  int nchunk;
+  int nchunk;             // forward: chunks; adjoint: chunks per channel
   const float2 *coef;     // adjoint: [T][form_coef_stride(S)] coefficients, offsets applied,
                           // column layout of form_col0
   double2 *part_fwd;      // [chunk][T * B]
-  double *part_adj;       // [chunk][Jpad]
+  double *part_adj;       // [channel][chunk][Jpad]
   unsigned long long *counter;
   int *err;
 };
