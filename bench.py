@@ -413,9 +413,9 @@ def run_formation(args, rank, world, local_rank):
     fwd_s = statistics.mean(e[0].elapsed_time(e[1]) for e in ev) / 1e3
     adj_s = statistics.mean(e[2].elapsed_time(e[3]) for e in ev) / 1e3
     plan.forward_formation(g.sky)
-    ev_f, _mx, tot = plan.last_stats()
+    ev_f, mx_f, tot = plan.last_stats()
     plan.adjoint_formation(coef, scale=2.0, mask=cfg.imaging_mask)
-    ev_a, _mx, _ = plan.last_stats()
+    ev_a, mx_a, _ = plan.last_stats()
     # parity of this step against the direct kernels on the same plan
     Vd = plan.forward(g.sky).to(torch.complex128)
     Vf = plan.forward_formation(g.sky).to(torch.complex128)
@@ -494,6 +494,8 @@ def run_formation(args, rank, world, local_rank):
                      "traffic_unit": "bytes per launch",
                      "traffic_source": FORM_NCU_TRAFFIC_SOURCE if args.workload in FORM_NCU_TRAFFIC else None},
         "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
+        "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_general_path": round(mx_f / tot, 4),
+                    "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_general_path": round(mx_a / tot, 4)},
         "forward_rel_l2_vs_direct": float(f"{rel_v:.3e}"),
         "gpu_launches": 10 * args.steps,
         "clocks": clk,
@@ -912,7 +914,8 @@ def main():
             f = run_formation(args, rank, world, local_rank)
             if res is not None and f is not None:
                 res["formation_mode"] = {k: f[k] for k in ("value", "unit", "ms_per_step", "e2e", "roofline",
-                                                           "kernel_ms", "forward_rel_l2_vs_direct", "clocks")}
+                                                           "kernel_ms", "culling", "forward_rel_l2_vs_direct",
+                                                           "clocks")}
                 res["formation_mode"]["entry_points"] = ("viss_plan_set_formation, viss_forward_formation, "
                                                          "viss_adjoint_formation")
         if res is not None:

@@ -179,11 +179,12 @@ int viss_plan_set_formation(viss_plan *plan, int64_t T, int S, const double *U, 
  * Each channel has its own sky and image; one launch per kernel covers all.
  * Reset to 1 by viss_plan_set_formation. */
 int viss_plan_set_formation_channels(viss_plan *plan, int channels);
-/* V (T x S(S-1)/2 complex64) for sky (C x J FP32); flags VISS_NO_MASK, VISS_ACCUMULATE. */
+/* V (T x S(S-1)/2 complex64) for sky (C x J FP32); flags VISS_NO_MASK,
+ * VISS_NO_OFFSET, VISS_ACCUMULATE (VISS_FP64 is rejected). */
 int viss_forward_formation(viss_plan *plan, const float *sky, float *V, int flags, void *stream);
 /* image (C x J FP32) = scale * the adjoint of the formation's samples for coef
  * (T x S(S-1)/2 complex64), each channel's samples into its own image;
- * flags VISS_NO_MASK, VISS_ACCUMULATE. */
+ * flags VISS_NO_MASK, VISS_NO_OFFSET, VISS_ACCUMULATE (VISS_FP64 is rejected). */
 int viss_adjoint_formation(viss_plan *plan, const float *coef, float *image, float scale, int flags,
                            void *stream);
 

@@ -148,3 +148,25 @@ def test_formation_channels(oracle, cuda_device):
     plan.set_formation(Us[0], None, occ_sat, occ_snap)
     V0 = plan.forward_formation(skies[0]).cpu().numpy()
     assert rel_l2(V0, V[0]) <= 1e-6
+
+
+def test_formation_flags(oracle, cuda_device):
+    """VISS_NO_OFFSET drops the phase offsets, VISS_ACCUMULATE adds into out,
+    as in the direct entry points."""
+    cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], nside=16, n_snap=16, n_sat=6)
+    obs, g, off = _case(cfg, 1e7, cuda_device, seed_off=9)
+    lmn, uvw, occ = g.lmn.cpu().numpy(), g.uvw.cpu().numpy(), g.occ.cpu().numpy()
+    sky64 = g.sky.cpu().numpy().astype(np.float64)
+    Vn = g.plan.forward_formation(g.sky, use_offset=False).cpu().numpy()
+    assert rel_l2(Vn, oracle.forward(uvw, lmn, sky64, obs.refs, occ)) <= 1e-5
+    V = g.plan.forward_formation(g.sky)
+    out = V.clone()
+    g.plan.forward_formation(g.sky, out=out, accumulate=True)
+    assert rel_l2(out.cpu().numpy(), 2 * V.cpu().numpy()) <= 1e-6
+    a = torch.ones(cfg.n_samples, dtype=torch.complex64, device=cuda_device)
+    Cn = g.plan.adjoint_formation(a, use_offset=False).cpu().numpy()
+    assert rel_l2(Cn, oracle.adjoint(uvw, np.ones(cfg.n_samples, np.complex128), lmn, obs.refs, occ)) <= 1e-5
+    img = g.plan.adjoint_formation(a)
+    img2 = img.clone()
+    g.plan.adjoint_formation(a, out=img2, accumulate=True)
+    assert rel_l2(img2.cpu().numpy(), 2 * img.cpu().numpy()) <= 1e-6

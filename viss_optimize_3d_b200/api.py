@@ -266,7 +266,8 @@ class Plan:
         if C > 1:
             check(lib.viss_plan_set_formation_channels(self._h, C), "viss_plan_set_formation_channels")
 
-    def forward_formation(self, sky, mask: bool = True, out: torch.Tensor | None = None):
+    def forward_formation(self, sky, mask: bool = True, use_offset: bool = True,
+                          out: torch.Tensor | None = None, accumulate: bool = False):
         """V (T * B complex64) of the formation's samples (channel-major with
         channels: sky then holds C x J values)."""
         sky = _cuda(sky, torch.float32, self.device)
@@ -278,12 +279,12 @@ class Plan:
         elif (out.dtype != torch.complex64 or not out.is_contiguous() or out.numel() != n
               or out.device != self.device):
             raise ValueError(f"out must be a contiguous complex64 tensor of {n} values on {self.device}")
-        check(lib.viss_forward_formation(self._h, _p(sky), _p(out), 0 if mask else capi.VISS_NO_MASK,
+        check(lib.viss_forward_formation(self._h, _p(sky), _p(out), self._flags(False, mask, use_offset, accumulate),
                                          _stream(sky)), "viss_forward_formation")
         return out
 
-    def adjoint_formation(self, coef, scale: float = 1.0, mask: bool = True,
-                          out: torch.Tensor | None = None):
+    def adjoint_formation(self, coef, scale: float = 1.0, mask: bool = True, use_offset: bool = True,
+                          out: torch.Tensor | None = None, accumulate: bool = False):
         """img (J FP32, or C x J with channels) = scale * the adjoint of the
         formation's samples."""
         n = self.form_T * self.form_B
@@ -298,7 +299,7 @@ class Plan:
               or out.device != self.device):
             raise ValueError(f"out must be a contiguous float32 tensor of {nimg} values on {self.device}")
         check(lib.viss_adjoint_formation(self._h, _p(coef), _p(out), float(scale),
-                                         0 if mask else capi.VISS_NO_MASK, _stream(coef)),
+                                         self._flags(False, mask, use_offset, accumulate), _stream(coef)),
               "viss_adjoint_formation")
         return out
 

@@ -702,7 +702,8 @@ int viss_forward_formation(viss_plan *p, const float *sky, float *V, int flags, 
   fp.pix = p->pixsky;
   fp.part_fwd = static_cast<double2 *>(p->part);
   VISS_CUDA(viss::launch_form_forward(fp, p->form_S, nchunk, st), "viss_forward_formation: kernel");
-  VISS_CUDA(viss::launch_form_reduce_fwd(T * B, nchunk, fp.part_fwd, p->form_has_off ? p->form_off : nullptr,
+  const bool use_off = p->form_has_off && !(flags & VISS_NO_OFFSET);
+  VISS_CUDA(viss::launch_form_reduce_fwd(T * B, nchunk, fp.part_fwd, use_off ? p->form_off : nullptr,
                                          reinterpret_cast<float2 *>(V), (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_forward_formation: reduce");
   p->last_total = T * B * p->J;
@@ -719,8 +720,9 @@ int viss_adjoint_formation(viss_plan *p, const float *coef, float *image, float 
   const int CB = viss::form_coef_stride(p->form_S);
   if (int s = ensure(p->form_coef, p->form_coef_cap, sizeof(float2) * T * CB, "formation coefficients"))
     return s;
+  const bool use_off = p->form_has_off && !(flags & VISS_NO_OFFSET);
   VISS_CUDA(viss::launch_form_stage_coef(T, p->form_S, reinterpret_cast<const float2 *>(coef),
-                                         p->form_has_off ? p->form_off : nullptr, p->form_coef, st),
+                                         use_off ? p->form_off : nullptr, p->form_coef, st),
             "viss_adjoint_formation: coefficients");
   // chunks of each channel's snapshots: about 16 waves of CTAs in all, at
   // least 4 staging tiles per chunk

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
     }
   };
 
-  unsigned long long evaluated = 0;
+  unsigned long long evaluated = 0, mixed_terms = 0;
   int next = 0, since_fold = 0;
   for (int it = 0; it < ntile; ++it) {
     const int tt = t0 + it, stage = it % ST;
@@ -221,8 +221,12 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
     }
     // a pair needs both satellites: skip the tile unless two see some of it
     if (tok && !snap_hidden && S - __popc(hid) >= 2) {
-      if (mix | hid) form_fwd_tile<S, kMixed>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
-      else form_fwd_tile<S, kOpen>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
+      if (mix | hid) {
+        form_fwd_tile<S, kMixed>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
+        mixed_terms += static_cast<unsigned long long>(kTilePix) * B;
+      } else {
+        form_fwd_tile<S, kOpen>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
+      }
       evaluated += static_cast<unsigned long long>(kTilePix) * B;
     }
     ring_release(s_empty, stage);
@@ -233,7 +237,10 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
   }
   if (tid == 0) ring_drain<ST>(s_full, next);
   fold();
-  if (p.counter && lane == 0 && evaluated) atomicAdd(p.counter, evaluated);
+  if (p.counter && lane == 0) {
+    if (evaluated) atomicAdd(p.counter, evaluated);
+    if (mixed_terms) atomicAdd(p.counter + 2, mixed_terms);
+  }
   if (!tok) return;
   double2 *out = p.part_fwd + static_cast<long long>(blockIdx.y) * p.T * B + t * B;
 #pragma unroll
@@ -384,7 +391,7 @@ __global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams
 #pragma unroll
   for (int q = 0; q < P; ++q) ks[q] = kc[q] = 0.f;
   const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
-  unsigned long long evaluated = 0;
+  unsigned long long evaluated = 0, mixed_terms = 0;
   int next = 0;
   for (int it = 0; it < ntile; ++it) {
     const int stage = it % ST;
@@ -419,6 +426,7 @@ __global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams
       // two code paths only: a third (hidden satellites without mixed rows)
       // measured slower, the unrolled bodies competing for instruction cache
       if (mix | hid) {
+        mixed_terms += static_cast<unsigned long long>(32 * P) * form_pairs(S);
         form_adj_snapshot<S, P, kMixed>(g.U + k * S, g.coef + k * CB, g.rows + k * S, hid, mix, sx, sy, sz, Q);
         if ((mix >> S) & 1u) {
           const double4 re = p.snap_rows ? g.snap[k] : pass;
@@ -437,7 +445,10 @@ __global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams
     ring_release(s_empty, stage);
   }
   if (tid == 0) ring_drain<ST>(s_full, next);
-  if (p.counter && lane == 0 && evaluated) atomicAdd(p.counter, evaluated);
+  if (p.counter && lane == 0) {
+    if (evaluated) atomicAdd(p.counter, evaluated);
+    if (mixed_terms) atomicAdd(p.counter + 2, mixed_terms);
+  }
   if (!tile_ok) return;
   double *out = p.part_adj + static_cast<long long>(blockIdx.y) * p.Jpad;
 #pragma unroll
