@@ -61,7 +61,7 @@ MUFU_TERMS_PER_CLK_PER_SM = 8     # 16 MUFU results/clk/SM, sin + cos per term
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # tuned shapes, from the one-pass ncu capture of this bench command recorded in
 # profiles/dram_c3_10mhz.md; bench.py cannot read DRAM counters itself.
-NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 56217088 + 45796096, "k_adjoint": 60853248 + 45885696}}
+NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 56540672 + 45793024, "k_adjoint": 60630784 + 45324032}}
 NCU_TRAFFIC_SOURCE = "profiles/dram_c3_10mhz.md (ncu, one pass, full-size workload)"
 FORM_NCU_TRAFFIC = {"c3_10mhz": {"k_form_forward": 32984064 + 449792, "k_form_adjoint": 36857344 + 32256}}
 FORM_NCU_TRAFFIC_SOURCE = "profiles/launches_bench_formation_c3_10mhz.md (ncu, one pass, full-size workload)"
@@ -336,7 +336,7 @@ def run_ours(args, rank, world, local_rank):
         "fp64_path": fp64,
         "tuning": {"chosen": {"forward": shapes[0], "adjoint": shapes[1]},
                    "forward_shapes": "(samples/thread, CTAs/SM) = (4,2) (4,3) (2,3) (2,4)",
-                   "adjoint_shapes": "(pixels/lane, CTAs/SM) = (8,2) (8,3) (4,3) (4,4)", **sweep},
+                   "adjoint_shapes": "(pixels/lane, CTAs/SM), 128-thread CTAs = (8,4) (8,5) (4,5) (4,6)", **sweep},
         "clocks": clk,
     }
     if args.cpu_baseline:

@@ -722,12 +722,12 @@ __global__ void k_reduce_adj(long long J, long long Jpad, int nchunk, const doub
 namespace viss {
 
 constexpr int kFwdNT = 256;
-constexpr int kAdjNT = 256;
+constexpr int kAdjNT = 128;  // 4 warps: less coupling of uneven warps through the ring
 
 // Launch shapes the plan's tuner chooses among: forward (samples per thread,
 // CTAs per SM) and adjoint (pixels per lane, CTAs per SM).
 const FwdShape kFwdShapes[kNumFwdShapes] = {{4, 2}, {4, 3}, {2, 3}, {2, 4}};
-const AdjShape kAdjShapes[kNumAdjShapes] = {{8, 2}, {8, 3}, {4, 3}, {4, 4}};
+const AdjShape kAdjShapes[kNumAdjShapes] = {{8, 4}, {8, 5}, {4, 5}, {4, 6}};
 
 template <int R, int MINB, bool M, bool F>
 static cudaError_t fwd_inst(const FwdParams &p, int nchunk, cudaStream_t st) {
@@ -804,10 +804,10 @@ cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool maske
   if (p.K <= 0 || p.Jpad <= 0) return cudaSuccess;
   if (fp64) return masked ? adj_inst<4, 1, true, true>(p, nchunk, st) : adj_inst<4, 1, false, true>(p, nchunk, st);
   switch (shape) {
-    case 1: return adj_m<8, 3>(p, nchunk, masked, st);
-    case 2: return adj_m<4, 3>(p, nchunk, masked, st);
-    case 3: return adj_m<4, 4>(p, nchunk, masked, st);
-    default: return adj_m<8, 2>(p, nchunk, masked, st);
+    case 1: return adj_m<8, 5>(p, nchunk, masked, st);
+    case 2: return adj_m<4, 5>(p, nchunk, masked, st);
+    case 3: return adj_m<4, 6>(p, nchunk, masked, st);
+    default: return adj_m<8, 4>(p, nchunk, masked, st);
   }
 }
 
