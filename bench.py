@@ -710,10 +710,17 @@ def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
             occ = np.concatenate([occ, obs.earth_rows])
     sel = (lambda r, idx: None if r is None else r[idx])
     K, J = uvw.shape[0], lmn.shape[0]
-    # calibrate on a tiny slice
-    t0 = time.perf_counter()
-    O.forward(uvw[:cores], lmn, sky, sel(refs, slice(0, cores)), occ, nthreads=cores)
-    rate = cores * J / max(time.perf_counter() - t0, 1e-6)       # terms/s
+    # calibrate on slices that grow until one takes >= 0.5 s (a tiny slice
+    # measures thread start-up more than the sum)
+    n_cal = cores
+    while True:
+        t0 = time.perf_counter()
+        O.forward(uvw[:n_cal], lmn, sky, sel(refs, slice(0, n_cal)), occ, nthreads=cores)
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 or n_cal >= K:
+            break
+        n_cal = min(K, n_cal * 4)
+    rate = n_cal * J / max(dt, 1e-6)                              # terms/s
     n_f = int(max(cores, min(K, 0.5 * budget_s * rate / J)))
     n_a = int(max(cores, min(J, 0.5 * budget_s * rate / K)))
     rng = np.random.default_rng(0)
