@@ -107,9 +107,11 @@ def read_inputs(root: str, variant_10m: bool = True):
     return case
 
 
-def oracle_vissgen(case, blockage: bool, frequency: float = 1e7):
+def oracle_vissgen(case, blockage: bool, frequency: float = 1e7, dcf_shift: bool = False):
     """vissGen (vissgen3d_blockage.cu:195-563) for one day, FP64 oracle:
-    returns (V after the w-rotation, complex128 per row; Re C per pixel)."""
+    returns (V after the w-rotation, complex128 per row; Re C per pixel).
+    dcf_shift: the blockage program's shifted DCF (vissgen3d_blockage.cu:133-139,
+    dcf[k] from shell k+1 for 1 <= k < nr; dcf[nr] as un-shifted)."""
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
     from oracle import oracle as O
@@ -132,6 +134,9 @@ def oracle_vissgen(case, blockage: bool, frequency: float = 1e7):
     lam = np.float32(3e8 / np.float32(frequency))
     nr = int(np.ceil(np.float32(100e3) / lam * np.float32(2)))
     gs, _counts, dcf = O.dcf(case["bll"], nr, 1)
+    if dcf_shift:
+        dcf = dcf.copy()
+        dcf[1:nr] = dcf[2:nr + 1]
     V = O.wrot(w, V)
     dg = O.gamma_dg(case["uvw"][:, 2], case["bll"][:n])
     wt = O.weights(gs[:n], dg, dcf, nr)

@@ -52,6 +52,19 @@ def test_vissgen_10m(tmp_path, oracle, exe, blockage):
     assert "npix: 192" in stdout and "total time:" in stdout
 
 
+def test_ref_dcf_shift(tmp_path, oracle):
+    """--ref-dcf-shift: the blockage program's own (shifted) DCF table."""
+    case = refcase.make_case()
+    refcase.write_inputs(case, str(tmp_path), variant_10m=True)
+    os.makedirs(tmp_path / "3dblockage10M")
+    run("vissgen3d_blockage_10m", tmp_path, "--ref-dcf-shift")
+    C = np.loadtxt(tmp_path / "3dblockage10M" / "C1day1M.txt")
+    _, Co = refcase.oracle_vissgen(case, True, dcf_shift=True)
+    _, Cu = refcase.oracle_vissgen(case, True)
+    assert np.abs(C - Co).max() <= 2e-5 * np.abs(Co).max(), np.abs(C - Co).max()
+    assert np.abs(Co - Cu).max() > 1e-3 * np.abs(Cu).max()    # the shift is visible in the image
+
+
 def test_vissgen_1m_two_days(tmp_path, oracle):
     case = refcase.make_case()
     refcase.write_inputs(case, str(tmp_path), variant_10m=False)

@@ -57,6 +57,10 @@ struct Options {
   std::string out_dir = VISS_VARIANT_BLOCKAGE ? (VISS_VARIANT_10M ? "3dblockage10M/" : "3dblockage/")
                                               : (VISS_VARIANT_10M ? "3dnoblockage10M/" : "3dnoblockage/");
   bool fp64 = false;
+  // the blockage program's DCF (vissgen3d_blockage.cu:133-139): shell k gets
+  // shell k+1's density, dcf[k] = the un-shifted dcf[k+1] for 1 <= k < nr;
+  // its dcf[nr] reads past the reference's arrays and stays un-shifted here
+  bool ref_dcf_shift = false;
   int max_devices = VISS_VARIANT_10M ? 1 : 1 << 20;
 };
 
@@ -191,6 +195,13 @@ void run_day(int p, const Options &opt, const SkyInputs &sky, int nr, double thr
       std::cout << "Viss[" << i << "]: (" << Vh[i].real() << "," << Vh[i].imag() << ")" << std::endl;
     // shells + DCF (:447-486), un-shifted formula
     VCALL(viss_dcf(bll_index, d_bll, nr, 1, d_gs, d_counts, d_dcf, nullptr));
+    if (opt.ref_dcf_shift && nr > 1) {
+      float *d_tmp = nullptr;
+      CUCALL(cudaMalloc(&d_tmp, sizeof(float) * (nr - 1)));
+      CUCALL(cudaMemcpy(d_tmp, d_dcf + 2, sizeof(float) * (nr - 1), cudaMemcpyDeviceToDevice));
+      CUCALL(cudaMemcpy(d_dcf + 1, d_tmp, sizeof(float) * (nr - 1), cudaMemcpyDeviceToDevice));
+      CUCALL(cudaFree(d_tmp));
+    }
     std::cout << "Period " << p + 1 << " calculateDcf..." << std::endl;
     // viss_gamma_trans (:494): w-rotation of every row, dg, and the clamped weights (:178,187)
     VCALL(viss_wrot(n, d_w, d_V, nullptr));
@@ -314,6 +325,7 @@ int main(int argc, char **argv) {
     else if (a == "--data-dir") opt.data_dir = val("--data-dir");
     else if (a == "--out-dir") opt.out_dir = val("--out-dir");
     else if (a == "--fp64") opt.fp64 = true;
+    else if (a == "--ref-dcf-shift") opt.ref_dcf_shift = true;
     else if (a == "--devices") opt.max_devices = std::atoi(val("--devices").c_str());
     else {
       std::fprintf(stderr, "unknown option %s\n", a.c_str());
