@@ -27,7 +27,9 @@ def _fmt(x) -> str:
     return repr(float(np.float32(x)))
 
 
-def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10):
+def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10,
+              spacing=(40.0, 250.0), cross_sigma: float = 30.0):
+    """spacing: along-track gaps U(lo, hi) m; cross_sigma: cross-track jitter (m)."""
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
     from oracle import oracle as O
@@ -47,8 +49,8 @@ def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10):
         e1 = np.array([1.0, 0.0, 0.0])
         e2 = np.array([0.0, math.cos(inc), math.sin(inc)])
         nrm = np.cross(e1, e2)
-        along = np.concatenate([[0.0], np.cumsum(rng.uniform(40.0, 250.0, n_sat - 1))])
-        cross = rng.normal(0.0, 30.0, n_sat)
+        along = np.concatenate([[0.0], np.cumsum(rng.uniform(spacing[0], spacing[1], n_sat - 1))])
+        cross = rng.normal(0.0, cross_sigma, n_sat)
         t = np.arange(n_snap) * (2 * math.pi / 40.0) + rng.uniform(0, 2 * math.pi)
         ang = t[:, None] + along[None, :] / r0
         P = r0 * (np.cos(ang)[..., None] * e1 + np.sin(ang)[..., None] * e2) + cross[None, :, None] * nrm

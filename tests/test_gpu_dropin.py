@@ -53,8 +53,11 @@ def test_vissgen_10m(tmp_path, oracle, exe, blockage):
 
 
 def test_ref_dcf_shift(tmp_path, oracle):
-    """--ref-dcf-shift: the blockage program's own (shifted) DCF table."""
-    case = refcase.make_case()
+    """--ref-dcf-shift: the blockage program's own (shifted) DCF table.  A
+    compact formation (baselines of 1-3 wavelengths) over 40 snapshots fills
+    the inner shells, so the weights sit below the 1/8 clamp and the shift
+    shows in the image."""
+    case = refcase.make_case(n_snap=40, spacing=(5.0, 20.0), cross_sigma=5.0)
     refcase.write_inputs(case, str(tmp_path), variant_10m=True)
     os.makedirs(tmp_path / "3dblockage10M")
     run("vissgen3d_blockage_10m", tmp_path, "--ref-dcf-shift")
