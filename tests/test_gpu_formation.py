@@ -86,6 +86,18 @@ def test_formation_rejects_invalid_use(cuda_device):
     U[1, 2, 0] = float("nan")
     with pytest.raises(VissError, match="non-finite"):
         plan.set_formation(U)
+    # shapes: U must be (T, S, 3) or (C, T, S, 3); occulter rows cover T snapshots
+    with pytest.raises(ValueError, match="U must be"):
+        plan.set_formation(torch.zeros((3, 4, 2), dtype=torch.float64))
+    with pytest.raises(ValueError, match="occulter rows must cover"):
+        plan.set_formation(torch.zeros((2, 3, 4, 3), dtype=torch.float64),
+                           occ_sat=torch.zeros((4, 4, 4), dtype=torch.float64))
+    plan.set_formation(torch.zeros((2, 3, 4, 3), dtype=torch.float64))
+    assert plan.form_C == 2 and plan.form_T == 6
+    with pytest.raises(ValueError, match="sky must hold"):
+        plan.forward_formation(torch.ones(lmn.shape[0], device=cuda_device))
+    with pytest.raises(ValueError, match="coef must hold"):
+        plan.adjoint_formation(torch.ones(5, dtype=torch.complex64, device=cuda_device))
 
 
 def test_formation_hidden_snapshots(oracle, cuda_device):
