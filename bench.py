@@ -42,6 +42,9 @@ WORKLOAD_TEXT = {
                 "10 MHz, Moon + Earth occultation",
     "c3_1mhz": "Nside 256 (786,432 px) x 388,800 uvw samples (45 baselines x 8,640 snapshots), "
                "1 MHz, Moon + Earth occultation",
+    "prod_1mhz": "production operating point at 1 MHz: Nside 512 (3,145,728 px) x 2,000,160 uvw samples "
+                 "(45 baselines x 44,448 snapshots, one day's 4,000,320 rows with the mirror rows folded), "
+                 "Moon + Earth occultation",
     "c2": "Nside 64 (49,152 px) x 20,160 uvw samples (28 baselines x 720 snapshots), 10 MHz, "
           "Moon occultation (profiling-size case)",
     "c3_small": "Nside 256 (786,432 px) x 48,600 uvw samples (45 baselines x 1,080 snapshots), "
@@ -58,13 +61,98 @@ WORKLOAD_TEXT = {
 METRIC = "G uvw x pixel terms/s (vis-gen + adjoint), split precision, rel-L2<=1e-5 vs FP64"
 UNIT = "Gterms/s"
 MUFU_TERMS_PER_CLK_PER_SM = 8     # 16 MUFU results/clk/SM, sin + cos per term
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# tuned shapes, from the one-pass ncu capture of this bench command recorded in
-# profiles/dram_c3_10mhz.md; bench.py cannot read DRAM counters itself.
-NCU_TRAFFIC = {"c3_10mhz": {"k_forward": 56540672 + 45793024, "k_adjoint": 60630784 + 45324032}}
-NCU_TRAFFIC_SOURCE = "profiles/dram_c3_10mhz.md (ncu, one pass, full-size workload)"
-FORM_NCU_TRAFFIC = {"c3_10mhz": {"k_form_forward": 32984064 + 449792, "k_form_adjoint": 36857344 + 32256}}
-FORM_NCU_TRAFFIC_SOURCE = "profiles/launches_bench_formation_c3_10mhz.md (ncu, one pass, full-size workload)"
+KERNEL_SOURCES = os.path.join(ROOT, "viss_optimize_3d_b200", "csrc")
+TRAFFIC_RECORD = os.path.join(ROOT, "viss_optimize_3d_b200", "ncu_traffic.json")
+# workloads too large for the launch-shape sweep, the FP64 comparison and the
+# formation comparison in a bench run of a few minutes
+BIG_WORKLOADS = ("prod_1mhz",)
+
+
+def kernel_sources_sha() -> str:
+    """sha256 over the CUDA sources (csrc/*.cu, *.cuh) in name order: the key
+    under which a measured DRAM traffic record is valid."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(KERNEL_SOURCES)):
+        if name.endswith((".cu", ".cuh")):
+            h.update(name.encode())
+            with open(os.path.join(KERNEL_SOURCES, name), "rb") as f:
+                h.update(f.read())
+    return h.hexdigest()
+
+
+def measured_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of `kernel` on `workload` from an ncu capture recorded by
+    `bench.py --record-traffic`, or None when no capture of the current
+    kernel sources exists (a record of other sources is never reported)."""
+    try:
+        with open(TRAFFIC_RECORD) as f:
+            rec = json.load(f)
+    except Exception:
+        return None, "no ncu traffic record"
+    if rec.get("kernel_sources_sha256") != kernel_sources_sha():
+        return None, "the ncu traffic record is of other kernel sources"
+    v = rec.get("bytes_per_launch", {}).get(workload, {}).get(kernel)
+    if v is None:
+        return None, f"no ncu traffic record of {kernel} on {workload}"
+    return v, f"ncu capture of these kernel sources (git {rec.get('git_commit', '?')}): {rec.get('command', '')}"
+
+
+def record_traffic(csv_path: str, workload: str, command: str):
+    """Write the DRAM traffic per launch of each kernel in an ncu --csv
+    metrics log (dram__bytes_read.sum, dram__bytes_write.sum) into the traffic
+    record, keyed by the current kernel sources' sha256."""
+    import csv
+    per = {}
+    with open(csv_path) as f:
+        lines = [ln for ln in f if ln.startswith('"')]
+    for row in csv.DictReader(lines):
+        name = row.get("Kernel Name", "")
+        metric, val = row.get("Metric Name"), row.get("Metric Value", "").replace(",", "")
+        if metric not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        unit = row.get("Metric Unit", "byte")
+        scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
+        for k in ("k_form_forward", "k_form_adjoint", "k_forward", "k_adjoint"):
+            if k + "<" in name or name.endswith(k):
+                per.setdefault(k, {}).setdefault(row.get("ID"), 0.0)
+                per[k][row.get("ID")] += float(val) * scale
+                break
+    try:
+        with open(TRAFFIC_RECORD) as f:
+            rec = json.load(f)
+    except Exception:
+        rec = {}
+    sha = kernel_sources_sha()
+    if rec.get("kernel_sources_sha256") != sha:
+        rec = {"kernel_sources_sha256": sha, "bytes_per_launch": {}}
+    try:
+        rec["git_commit"] = subprocess.run(["git", "rev-parse", "--short", "HEAD"], cwd=ROOT,
+                                           capture_output=True, text=True).stdout.strip() or "?"
+    except Exception:
+        rec["git_commit"] = "?"
+    rec["command"] = command
+    rec["bytes_per_launch"][workload] = {k: int(statistics.median(v.values())) for k, v in per.items()}
+    with open(TRAFFIC_RECORD, "w") as f:
+        json.dump(rec, f, indent=1)
+    return rec
+
+
+def bench_config(args, J: int, K: int, world: int) -> dict:
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD_TEXT.get(args.workload, args.workload)
+                        + ("; formation mode" if getattr(args, "formation", False) else ""),
+            "pixels": J, "samples": K, "terms_per_step": 2 * K * J,
+            "l2": "GPU arm: flushed between timed steps (256 MB write)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def workload_config(name: str):
+    from viss_optimize_3d_b200 import synth
+    if name == "c3_small":
+        return synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
+    return synth.CONFIGS[name]
 
 
 def peaks():
@@ -136,15 +224,14 @@ def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
     from viss_optimize_3d_b200 import api, pipeline, replicas, synth
+    from viss_optimize_3d_b200._capi import check, lib
+    import ctypes as C
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     if args.formation:
         return run_formation(args, rank, world, local_rank)
-    if args.workload == "c3_small":
-        cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
-    else:
-        cfg = synth.CONFIGS[args.workload]
+    cfg = workload_config(args.workload)
     if world > 1:
         import dataclasses
         # one observation day per replica, the reference's round-robin day split
@@ -157,6 +244,7 @@ def run_ours(args, rank, world, local_rank):
     terms_per_step = 2 * K * J
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+    big = args.workload in BIG_WORKLOADS
 
     # device-resident step: forward, DCF + weights, adjoint
     def step():
@@ -166,23 +254,29 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    # launch-shape sweep (recorded) and the plan's own tuner (chooses)
     V0 = g.plan.forward(g.sky)
     gs0, _c0, dcf0 = api.dcf(g.bll, g.nr, multiplicity=2)
     coef0 = api.scale_coef(api.weights(g.w, g.bll, gs0, dcf0, g.nr)[1], V0)
     sweep = {"forward_ms": [], "adjoint_ms": []}
-    for shape in range(4):
-        g.plan.set_shapes(shape, shape)
-        for key, fn in (("forward_ms", lambda: g.plan.forward(g.sky)),
-                        ("adjoint_ms", lambda: g.plan.adjoint(coef0, scale=2.0, mask=cfg.imaging_mask))):
-            fn()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            sweep[key].append(round(e0.elapsed_time(e1), 3))
-    shapes = g.plan.tune(g.sky, coef0, mask=cfg.imaging_mask)
+    if big:
+        # the shapes the tuner picks at the headline size; a sweep here would
+        # take longer than the timed run
+        g.plan.set_shapes(0, 0)
+        shapes = (0, 0)
+    else:
+        # launch-shape sweep (recorded) and the plan's own tuner (chooses)
+        for shape in range(4):
+            g.plan.set_shapes(shape, shape)
+            for key, fn in (("forward_ms", lambda: g.plan.forward(g.sky)),
+                            ("adjoint_ms", lambda: g.plan.adjoint(coef0, scale=2.0, mask=cfg.imaging_mask))):
+                fn()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                sweep[key].append(round(e0.elapsed_time(e1), 3))
+        shapes = g.plan.tune(g.sky, coef0, mask=cfg.imaging_mask)
     torch.cuda.synchronize()
     fwd_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
@@ -190,6 +284,11 @@ def run_ours(args, rank, world, local_rank):
               for _ in range(args.steps)]
     step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.steps)]
+    # this rank's day images summed on the device (FP64, non-finite as 0), and
+    # over the ranks by one NCCL all-reduce at the end of the timed region:
+    # the day-summed image of the reference's notebooks, replacing its
+    # round-robin days with a host sum (vissgen3d_blockage.cu:271-279)
+    day_sum = torch.zeros(J, dtype=torch.float64, device=dev)
     clocks = ClockSampler(local_rank)
     if world > 1:
         torch.distributed.barrier()
@@ -207,6 +306,9 @@ def run_ours(args, rank, world, local_rank):
         adj_ev[i][0].record(stream)
         img = g.plan.adjoint(coef, scale=2.0, mask=cfg.imaging_mask)
         adj_ev[i][1].record(stream)
+        replicas.add_day_image(day_sum, img)
+        if i == args.steps - 1:
+            replicas.sum_images(day_sum)
         step_ev[i][1].record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -216,41 +318,57 @@ def run_ours(args, rank, world, local_rank):
     fwd_ms = [a.elapsed_time(b) for a, b in fwd_ev]
     adj_ms = [a.elapsed_time(b) for a, b in adj_ev]
     total_s = sum(step_ms) / 1e3
-    # culled fraction of the last forward/adjoint (device counters)
+    # culled fraction of the last forward/adjoint (device counters); also
+    # raises if a bounded device-side wait gave up in either kernel
     g.plan.forward(g.sky)
     ev_f, mx_f, tot = g.plan.last_stats()
     g.plan.adjoint(coef, scale=2.0, mask=cfg.imaging_mask)
     ev_a, mx_a, _ = g.plan.last_stats()
+    day_sum_ok = bool(torch.isfinite(day_sum).all().item())
 
-    # end to end through the public API from pinned host buffers
+    # end to end through the public API from pinned host buffers: every step
+    # uploads a new observation's inputs (sky, uvw, satellite positions, the
+    # Earth rows, occulter refs), builds the occulter rows on the device
+    # (viss_occulters), stages the samples, runs forward + DCF + adjoint and
+    # reads V and the image back
     sky_h = torch.from_numpy(obs.sky_at(f_hz).astype(np.float32) * np.float32(4 * math.pi / J)).pin_memory()
     uvw_h = torch.from_numpy(obs.uvw(f_hz)).pin_memory()
     masked = obs.refs is not None
     refs_h = torch.from_numpy(obs.refs).pin_memory() if masked else None
+    P_h = torch.from_numpy(np.ascontiguousarray(obs.occ_sat_positions)).pin_memory() if masked else None
+    earth_h = (torch.from_numpy(np.ascontiguousarray(obs.earth_rows)).pin_memory()
+               if masked and obs.earth_rows is not None else None)
     img_h = torch.empty(J, dtype=torch.float32).pin_memory()
     V_h = torch.empty(K, dtype=torch.complex64).pin_memory()
     sky_d = torch.empty_like(g.sky)
     uvw_d = torch.empty_like(g.uvw)
     refs_d = torch.empty_like(g.refs) if masked else None
-    from viss_optimize_3d_b200._capi import check, lib
-    import ctypes as C
+    P_d = torch.empty(P_h.shape, dtype=torch.float64, device=dev) if masked else None
+    occ_d = torch.empty_like(g.occ) if masked else None
+    n_sat_rows = P_h.shape[0] if masked else 0
 
     def e2e_step():
         sky_d.copy_(sky_h, non_blocking=True)
         uvw_d.copy_(uvw_h, non_blocking=True)
+        st = C.c_void_p(stream.cuda_stream)
         if masked:
             refs_d.copy_(refs_h, non_blocking=True)
+            P_d.copy_(P_h, non_blocking=True)
+            check(lib.viss_occulters(n_sat_rows, C.c_void_p(P_d.data_ptr()), synth.R_MOON, 0, 0.0,
+                                     C.c_void_p(occ_d.data_ptr()), st), "viss_occulters")
+            if earth_h is not None:
+                occ_d[n_sat_rows:].copy_(earth_h, non_blocking=True)
         check(lib.viss_plan_set_samples(g.plan._h, K, C.c_void_p(uvw_d.data_ptr()), None,
                                         C.c_void_p(refs_d.data_ptr()) if masked else None,
-                                        g.occ.shape[0] if masked else 0,
-                                        C.c_void_p(g.occ.data_ptr()) if masked else None,
-                                        C.c_void_p(stream.cuda_stream)), "set_samples")
+                                        occ_d.shape[0] if masked else 0,
+                                        C.c_void_p(occ_d.data_ptr()) if masked else None, st),
+              "set_samples")
         Vd = g.plan.forward(sky_d)
         imgd = pipeline.dirty_image(g, Vd)
         V_h.copy_(Vd, non_blocking=True)
         img_h.copy_(imgd, non_blocking=True)
 
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = 1 if big else max(1, min(args.steps, 3))
     e2e_step()
     torch.cuda.synchronize()
     if world > 1:
@@ -262,7 +380,9 @@ def run_ours(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_s = e0.elapsed_time(e1) / 1e3
-    h2d = J * 4 + K * 24 + (K * 12 if masked else 0)
+    h2d = J * 4 + K * 24
+    if masked:
+        h2d += K * 12 + P_h.numel() * 8 + (earth_h.numel() * 8 if earth_h is not None else 0)
     d2h = J * 4 + K * 8
 
     # max over ranks (device-timed seconds)
@@ -270,22 +390,32 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return None
 
-    # the plain FP64 path on the same step (the split path's >= 3x target)
+    # the plain FP64 path on the same step (the split path's >= 3x target):
+    # one warm-up, then the mean of three timed repeats
     fp64 = None
-    if args.fp64_compare:
-        f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        f0.record(stream)
-        Vd = g.plan.forward(g.sky, fp64=True)
-        f1.record(stream)
+    if args.fp64_compare and not big:
+        reps = 3
+        g.plan.forward(g.sky, fp64=True)
         g.plan.adjoint(coef, scale=2.0, mask=cfg.imaging_mask, fp64=True)
-        f2.record(stream)
         torch.cuda.synchronize()
-        fp64_fwd, fp64_adj = f0.elapsed_time(f1) / 1e3, f1.elapsed_time(f2) / 1e3
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(reps)]
+        for r in range(reps):
+            flush.fill_(float(r))
+            ev[r][0].record(stream)
+            Vd = g.plan.forward(g.sky, fp64=True)
+            ev[r][1].record(stream)
+            g.plan.adjoint(coef, scale=2.0, mask=cfg.imaging_mask, fp64=True)
+            ev[r][2].record(stream)
+        torch.cuda.synchronize()
+        g.plan.last_stats()
+        fp64_fwd = statistics.mean(e[0].elapsed_time(e[1]) for e in ev) / 1e3
+        fp64_adj = statistics.mean(e[1].elapsed_time(e[2]) for e in ev) / 1e3
         split_fwd, split_adj = statistics.mean(fwd_ms) / 1e3, statistics.mean(adj_ms) / 1e3
         Vs = g.plan.forward(g.sky).to(torch.complex128)
         rel = (torch.linalg.norm(Vs - Vd.to(torch.complex128)) / torch.linalg.norm(Vd.to(torch.complex128))).item()
         fp64 = {"value": round(terms_per_step / (fp64_fwd + fp64_adj) / 1e9, 3), "unit": UNIT,
                 "forward_ms": round(fp64_fwd * 1e3, 2), "adjoint_ms": round(fp64_adj * 1e3, 2),
+                "timed_repeats": reps, "warmup": 1,
                 "split_speedup": round((fp64_fwd + fp64_adj) / (split_fwd + split_adj), 2),
                 "forward_rel_l2_split_vs_fp64": float(f"{rel:.3e}")}
 
@@ -299,6 +429,13 @@ def run_ours(args, rank, world, local_rank):
     dom_eval = (ev_f if dom == "forward" else ev_a)
     achieved = K * J / dom_s
     value = terms_per_step * args.steps * world / total_s / 1e9
+    G = g.occ.shape[0] if g.occ is not None else 0
+    # algorithmic bytes of one launch: each input record read once, each
+    # output written once (pixel records 32 B, sample records 32 B + refs
+    # 16 B, occulter rows 32 B + 16 B, V 8 B / coefficients 8 B, image 4 B)
+    alg_bytes = {"forward": J * 32 + K * 48 + G * 48 + K * 8,
+                 "adjoint": J * 32 + K * 48 + G * 48 + K * 8 + J * 4}[dom]
+    traffic, traffic_src = measured_traffic(args.workload, f"k_{dom}")
     res = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -312,31 +449,32 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64-phase/f32-sincos",
         "data": "synthetic (seeded lunar-orbit formation and log-normal sky, see synth.py)",
-        "config": {"workload": WORKLOAD_TEXT.get(args.workload, args.workload),
-                   "pixels": J, "samples": K, "terms_per_step": terms_per_step,
-                   "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": bench_config(args, J, K, world),
         "e2e": {"value": round(terms_per_step * e2e_steps / e2e_s / 1e9 * world, 3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "path": "pinned host sky/uvw/refs -> viss_plan_set_samples -> viss_forward -> "
-                        "viss_dcf/viss_weights -> viss_adjoint -> pinned host V/image"},
+                "path": "pinned host sky/uvw/refs/satellite positions/Earth rows -> viss_occulters -> "
+                        "viss_plan_set_samples -> viss_forward -> viss_dcf/viss_weights -> viss_adjoint "
+                        "-> pinned host V/image"},
         "roofline": {"bound": "sfu", "kernel": f"k_{dom}",
                      "achieved": round(achieved / 1e9, 2), "peak": round(peak_terms / 1e9, 1),
                      "unit": "Gterms/s", "frac": round(achieved / peak_terms, 4),
                      "peak_source": f"8 terms/clk/SM x {nsm} SMs x sm_max_mhz ({pk_kind})",
                      "evaluated_frac": round(dom_eval / (K * J), 4),
                      "frac_of_evaluated": round(dom_eval / dom_s / peak_terms, 4),
-                     "traffic": NCU_TRAFFIC.get(args.workload, {}).get(f"k_{dom}"),
-                     "traffic_unit": "bytes per launch",
-                     "traffic_source": NCU_TRAFFIC_SOURCE if args.workload in NCU_TRAFFIC else None},
+                     "algorithmic_bytes": alg_bytes,
+                     "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
+                     "traffic_source": traffic_src},
         "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
         "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_mixed": round(mx_f / tot, 4),
                     "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_mixed": round(mx_a / tot, 4)},
-        "gpu_launches": 10 * args.steps,
+        "day_sum": {"ranks": world, "reduction": "NCCL all-reduce (SUM) of the FP64 day sums"
+                    if world > 1 else "single rank: device day sum only", "finite": day_sum_ok},
+        "gpu_launches": 11 * args.steps,
         "fp64_path": fp64,
         "tuning": {"chosen": {"forward": shapes[0], "adjoint": shapes[1]},
                    "forward_shapes": "(samples/thread, CTAs/SM) = (4,2) (4,3) (2,3) (2,4)",
-                   "adjoint_shapes": "(pixels/lane, CTAs/SM), 128-thread CTAs = (8,4) (8,5) (4,5) (4,6)", **sweep},
+                   "adjoint_shapes": "(pixels/lane, CTAs/SM), 128-thread CTAs = (8,4) (8,5) (4,5) (4,6)",
+                   **({"note": "fixed at the headline size's choice (no sweep at this size)"} if big else sweep)},
         "clocks": clk,
     }
     if args.cpu_baseline:
@@ -359,10 +497,8 @@ def run_formation(args, rank, world, local_rank):
     import ctypes as C
 
     dev = torch.device("cuda", local_rank)
-    if args.workload == "c3_small":
-        cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
-    elif args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz"):
-        cfg = synth.CONFIGS[args.workload]
+    if args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz", "c3_small", "prod_1mhz"):
+        cfg = workload_config(args.workload)
     else:
         raise SystemExit(f"--formation covers the single-channel workloads, not {args.workload}")
     if world > 1:
@@ -421,27 +557,41 @@ def run_formation(args, rank, world, local_rank):
     Vf = plan.forward_formation(g.sky).to(torch.complex128)
     rel_v = (torch.linalg.norm(Vf - Vd) / torch.linalg.norm(Vd)).item()
 
-    # end to end: pinned host sky and satellite vectors -> image and V on the host
+    # end to end: every step uploads a new observation's inputs from pinned
+    # host memory (sky, satellite positions, the Earth rows), forms the
+    # satellite vectors U = (P - centre) / lambda and the Moon occulter rows
+    # (viss_occulters) on the device, stages the formation, runs forward +
+    # DCF + adjoint and reads V and the image back
     sky_h = torch.from_numpy(obs.sky_at(f_hz).astype(np.float32) * np.float32(4 * math.pi / J)).pin_memory()
-    U_h = U.cpu().pin_memory()
-    U_d, sky_d = torch.empty_like(U), torch.empty_like(g.sky)
+    P_h = torch.from_numpy(np.ascontiguousarray(obs.positions, dtype=np.float64)).pin_memory()
+    earth_h = torch.from_numpy(np.ascontiguousarray(obs.earth_rows)).pin_memory() if occ_snap is not None else None
+    P_d, sky_d = torch.empty(P_h.shape, dtype=torch.float64, device=dev), torch.empty_like(g.sky)
+    osat_d = torch.empty_like(occ_sat) if occ_sat is not None else None
+    osnap_d = torch.empty_like(occ_snap) if occ_snap is not None else None
     img_h = torch.empty(J, dtype=torch.float32).pin_memory()
     V_h = torch.empty(K, dtype=torch.complex64).pin_memory()
-    os_p = C.c_void_p(occ_sat.data_ptr()) if occ_sat is not None else None
-    on_p = C.c_void_p(occ_snap.data_ptr()) if occ_snap is not None else None
+    lam = synth.C_LIGHT / f_hz
 
     def e2e_step():
+        st = C.c_void_p(stream.cuda_stream)
         sky_d.copy_(sky_h, non_blocking=True)
-        U_d.copy_(U_h, non_blocking=True)
+        P_d.copy_(P_h, non_blocking=True)
+        U_d = ((P_d - P_d.mean(dim=1, keepdim=True)) / lam).contiguous()
+        if osat_d is not None:
+            check(lib.viss_occulters(P_d.shape[0] * P_d.shape[1], C.c_void_p(P_d.data_ptr()), synth.R_MOON,
+                                     0, 0.0, C.c_void_p(osat_d.data_ptr()), st), "viss_occulters")
+        if osnap_d is not None:
+            osnap_d.copy_(earth_h, non_blocking=True)
         check(lib.viss_plan_set_formation(plan._h, plan.form_T, plan.form_S, C.c_void_p(U_d.data_ptr()),
-                                          None, os_p, on_p, C.c_void_p(stream.cuda_stream)),
+                                          None, None if osat_d is None else C.c_void_p(osat_d.data_ptr()),
+                                          None if osnap_d is None else C.c_void_p(osnap_d.data_ptr()), st),
               "viss_plan_set_formation")
         Vd_ = plan.forward_formation(sky_d)
         imgd = image(Vd_)
         V_h.copy_(Vd_, non_blocking=True)
         img_h.copy_(imgd, non_blocking=True)
 
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = 1 if args.workload in BIG_WORKLOADS else max(1, min(args.steps, 3))
     e2e_step()
     torch.cuda.synchronize()
     if world > 1:
@@ -453,9 +603,11 @@ def run_formation(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_s = e0.elapsed_time(e1) / 1e3
+    h2d = J * 4 + P_h.numel() * 8 + (earth_h.numel() * 8 if earth_h is not None else 0)
     total_s, e2e_s = replicas.max_over_ranks([total_s, e2e_s], device=dev)
     if rank != 0:
         return None
+    traffic, traffic_src = measured_traffic(args.workload, "k_form_forward" if fwd_s >= adj_s else "k_form_adjoint")
     pk, pk_kind = peaks()
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_terms = 128 / FORM_FFMA_PER_TERM * nsm * pk["sm_max_mhz"] * 1e6
@@ -476,13 +628,11 @@ def run_formation(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64-phase/f32-sincos/f32-pair-products",
         "data": "synthetic (seeded lunar-orbit formation and log-normal sky, see synth.py)",
-        "config": {"workload": WORKLOAD_TEXT.get(args.workload, args.workload) + "; formation mode",
-                   "pixels": J, "samples": K, "satellites": plan.form_S, "snapshots": plan.form_T,
-                   "terms_per_step": terms_per_step, "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": {**bench_config(args, J, K, world), "satellites": plan.form_S, "snapshots": plan.form_T},
         "e2e": {"value": round(terms_per_step * e2e_steps / e2e_s / 1e9 * world, 3), "unit": UNIT,
-                "h2d_bytes_per_step": J * 4 + U.numel() * 8, "d2h_bytes_per_step": J * 4 + K * 8,
-                "path": "pinned host sky/U -> viss_plan_set_formation -> viss_forward_formation -> "
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": J * 4 + K * 8,
+                "path": "pinned host sky/satellite positions/Earth rows -> U and viss_occulters on the "
+                        "device -> viss_plan_set_formation -> viss_forward_formation -> "
                         "viss_dcf/viss_weights -> viss_adjoint_formation -> pinned host V/image"},
         "roofline": {"bound": "fp32", "kernel": f"k_form_{dom}",
                      "achieved": round(achieved / 1e9, 2), "peak": round(peak_terms / 1e9, 1),
@@ -490,9 +640,8 @@ def run_formation(args, rank, world, local_rank):
                      "peak_source": f"128 FP32 lanes/clk/SM / {FORM_FFMA_PER_TERM} FFMA per term x {nsm} SMs "
                                     f"x sm_max_mhz ({pk_kind})",
                      "evaluated_frac": round(dom_eval / (K * J), 4),
-                     "traffic": FORM_NCU_TRAFFIC.get(args.workload, {}).get(f"k_form_{dom}"),
-                     "traffic_unit": "bytes per launch",
-                     "traffic_source": FORM_NCU_TRAFFIC_SOURCE if args.workload in FORM_NCU_TRAFFIC else None},
+                     "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
+                     "traffic_source": traffic_src},
         "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
         "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_general_path": round(mx_f / tot, 4),
                     "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_general_path": round(mx_a / tot, 4)},
@@ -690,54 +839,69 @@ def run_reconstruction(args):
 
 
 # ---------------------------------------------------------- CPU baseline
-def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
-    """The FP64 CPU restatement (oracle/) on all host cores, on a bounded
-    sample: n_f samples x all pixels (forward) and n_a pixels x all samples
-    (adjoint), sized to about budget_s seconds."""
-    import numpy as np
-    from oracle import oracle as O
+class CpuSampler:
+    """The FP64 CPU restatement (oracle/) on all host cores, timed on bounded
+    samples of a workload: n_f samples x all pixels (forward) and n_a pixels
+    x all samples (adjoint), sized from a calibrated rate to a time budget."""
 
-    O.build()
-    cores = O.max_threads()
-    _, _, xyz = O.pix2ang(obs.cfg.nside)
-    lmn = O.lmn_from_xyz(xyz)
-    uvw = obs.uvw(f_hz)
-    sky = obs.sky_at(f_hz) * (4 * math.pi / obs.cfg.npix)
-    refs, occ = obs.refs, None
-    if refs is not None:
-        occ = O.occulters(obs.occ_sat_positions, 1737.4e3, 0)
-        if obs.earth_rows is not None:
-            occ = np.concatenate([occ, obs.earth_rows])
-    sel = (lambda r, idx: None if r is None else r[idx])
-    K, J = uvw.shape[0], lmn.shape[0]
-    # calibrate on slices that grow until one takes >= 0.5 s (a tiny slice
-    # measures thread start-up more than the sum)
-    n_cal = cores
-    while True:
+    def __init__(self, obs, f_hz):
+        import numpy as np
+        from oracle import oracle as O
+
+        O.build()
+        self.O = O
+        self.cores = O.max_threads()
+        _, _, xyz = O.pix2ang(obs.cfg.nside)
+        self.lmn = O.lmn_from_xyz(xyz)
+        self.uvw = obs.uvw(f_hz)
+        self.sky = obs.sky_at(f_hz) * (4 * math.pi / obs.cfg.npix)
+        self.refs, self.occ = obs.refs, None
+        if self.refs is not None:
+            self.occ = O.occulters(obs.occ_sat_positions, 1737.4e3, 0)
+            if obs.earth_rows is not None:
+                self.occ = np.concatenate([self.occ, obs.earth_rows])
+        self.K, self.J = self.uvw.shape[0], self.lmn.shape[0]
+        # calibrate on slices that grow until one takes >= 0.5 s (a tiny slice
+        # measures thread start-up more than the sum)
+        n_cal = self.cores
+        while True:
+            t0 = time.perf_counter()
+            O.forward(self.uvw[:n_cal], self.lmn, self.sky, self._sel(slice(0, n_cal)), self.occ,
+                      nthreads=self.cores)
+            dt = time.perf_counter() - t0
+            if dt >= 0.5 or n_cal >= self.K:
+                break
+            n_cal = min(self.K, n_cal * 4)
+        self.rate = n_cal * self.J / max(dt, 1e-6)            # terms/s
+
+    def _sel(self, idx):
+        return None if self.refs is None else self.refs[idx]
+
+    def sample(self, budget_s: float, seed: int = 0) -> dict:
+        import numpy as np
+        K, J, cores = self.K, self.J, self.cores
+        n_f = int(max(cores, min(K, 0.5 * budget_s * self.rate / J)))
+        n_a = int(max(cores, min(J, 0.5 * budget_s * self.rate / K)))
+        rng = np.random.default_rng(seed)
+        ks = np.sort(rng.choice(K, n_f, replace=False))
+        js = np.sort(rng.choice(J, n_a, replace=False))
+        a = np.ones(K, dtype=np.complex128)
         t0 = time.perf_counter()
-        O.forward(uvw[:n_cal], lmn, sky, sel(refs, slice(0, n_cal)), occ, nthreads=cores)
-        dt = time.perf_counter() - t0
-        if dt >= 0.5 or n_cal >= K:
-            break
-        n_cal = min(K, n_cal * 4)
-    rate = n_cal * J / max(dt, 1e-6)                              # terms/s
-    n_f = int(max(cores, min(K, 0.5 * budget_s * rate / J)))
-    n_a = int(max(cores, min(J, 0.5 * budget_s * rate / K)))
-    rng = np.random.default_rng(0)
-    ks = np.sort(rng.choice(K, n_f, replace=False))
-    js = np.sort(rng.choice(J, n_a, replace=False))
-    a = np.ones(K, dtype=np.complex128)
-    t0 = time.perf_counter()
-    O.forward(uvw[ks], lmn, sky, sel(refs, ks), occ, nthreads=cores)
-    t1 = time.perf_counter()
-    O.adjoint(uvw, a, lmn[js], refs, occ, nthreads=cores)
-    t2 = time.perf_counter()
-    terms = n_f * J + n_a * K
-    return {"value": round(terms / (t2 - t0) / 1e9, 5), "unit": UNIT, "cores": cores,
-            "kind": "port",
-            "sample": f"{n_f} samples x {J} pixels (forward) + {n_a} pixels x {K} samples "
-                      f"(adjoint), FP64 oracle, OpenMP",
-            "seconds": round(t2 - t0, 2)}
+        self.O.forward(self.uvw[ks], self.lmn, self.sky, self._sel(ks), self.occ, nthreads=cores)
+        t1 = time.perf_counter()
+        self.O.adjoint(self.uvw, a, self.lmn[js], self.refs, self.occ, nthreads=cores)
+        t2 = time.perf_counter()
+        return {"terms": n_f * J + n_a * K, "seconds": t2 - t0,
+                "sample": f"{n_f} samples x {J} pixels (forward) + {n_a} pixels x {K} samples "
+                          f"(adjoint), FP64 oracle, OpenMP"}
+
+
+def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
+    """One bounded sample of the workload through the FP64 CPU restatement."""
+    smp = CpuSampler(obs, f_hz)
+    r = smp.sample(budget_s)
+    return {"value": round(r["terms"] / r["seconds"] / 1e9, 5), "unit": UNIT, "cores": smp.cores,
+            "kind": "port", "sample": r["sample"], "seconds": round(r["seconds"], 2)}
 
 
 # ---------------------------------------------------------- reference arm
@@ -830,39 +994,42 @@ def run_stream(args):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's path on the host cores.  The
+    reference has no CPU implementation (its kernels are CUDA only), so this
+    is the FP64 restatement of its kernels (oracle/) on every host thread.
+    Each step is one bounded sample of the workload (a seeded subset of
+    samples x all pixels for the forward and of pixels x all samples for the
+    adjoint), sized so that warm-up + timed steps take about
+    --reference-seconds in all; ms_per_step is the measured time of one such
+    sample and value the terms it evaluated per second."""
     if rank != 0:
         return None
     from viss_optimize_3d_b200 import synth
-    if args.workload == "c3_small":
-        cfg = synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
-    elif args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz"):
-        cfg = synth.CONFIGS[args.workload]
+    if args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz", "c3_small", "prod_1mhz"):
+        cfg = workload_config(args.workload)
     else:
         return {"impl": "reference", "unavailable": f"workload {args.workload} has no reference "
                 "counterpart (batched channels, reconstruction and day files are this repository's)"}
     obs = synth.make_observation(cfg)
     f_hz = cfg.freqs_hz[0]
-    vals = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(obs, f_hz, budget_s=args.cpu_seconds)
-        if i >= args.warmup:
-            vals.append(r)
-    v = statistics.mean(x["value"] for x in vals)
-    last = vals[-1]
-    terms = 2 * obs.cfg.n_samples * obs.cfg.npix
+    smp = CpuSampler(obs, f_hz)
+    budget = min(args.cpu_seconds, max(1.0, args.reference_seconds / max(1, args.steps + args.warmup)))
+    runs = [smp.sample(budget, seed=i) for i in range(args.warmup + args.steps)][args.warmup:]
+    terms = sum(r["terms"] for r in runs)
+    secs = sum(r["seconds"] for r in runs)
+    v = terms / secs / 1e9
     return {
         "impl": "reference",
         "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(terms / (v * 1e9) * 1e3, 1),
+        "ms_per_step": round(secs / len(runs) * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (same generator and seed as our arm)",
-        "config": {"workload": WORKLOAD_TEXT.get(args.workload, args.workload),
-                   "pixels": obs.cfg.npix, "samples": obs.cfg.n_samples, "terms_per_step": terms,
-                   "note": "the reference has no CPU implementation; this is the FP64 "
-                           "restatement of its kernels (oracle/), timed on a bounded sample"},
-        "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": last["cores"],
-                         "kind": "port", "sample": last["sample"]},
+        "config": bench_config(args, obs.cfg.npix, obs.cfg.n_samples, world),
+        "step": "one bounded sample of the workload per step (the reference has no CPU "
+                "implementation; this is the FP64 restatement of its kernels, oracle/)",
+        "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": smp.cores,
+                         "kind": "port", "sample": runs[-1]["sample"] + " per step"},
         "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -877,7 +1044,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false",
                     help="skip timing the plain FP64 path on the same step")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="time budget of the CPU baseline's bounded sample (and the cap per step of "
+                         "the reference arm)")
+    ap.add_argument("--reference-seconds", type=float, default=150.0,
+                    help="reference arm: about this many seconds for warm-up + timed steps in all")
+    ap.add_argument("--record-traffic", metavar="NCU_CSV",
+                    help="store the DRAM bytes per launch of an ncu --csv metrics log of this "
+                         "workload as the traffic record of the current kernel sources, and exit")
+    ap.add_argument("--record-command", default="", help="the ncu command line, stored with the record")
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOAD_TEXT),
                     help="benchmark configuration (default: the headline one)")
     ap.add_argument("--formation", action="store_true",
@@ -887,6 +1062,9 @@ def main():
     ap.add_argument("--stream-days", type=int, default=4,
                     help="days of the stream workload")
     args = ap.parse_args()
+    if args.record_traffic:
+        print(json.dumps(record_traffic(args.record_traffic, args.workload, args.record_command)))
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -915,7 +1093,7 @@ def main():
             print(json.dumps(run_stream(args)), flush=True)
             return
         res = run_ours(args, rank, world, local_rank)
-        if not args.formation and args.formation_compare and args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz", "c3_small"):
+        if not args.formation and args.formation_compare and args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz", "c3_small"):  # noqa: E501
             # the same step through the formation entry points (satellite vectors
             # instead of per-sample uvw), reported beside the headline
             f = run_formation(args, rank, world, local_rank)

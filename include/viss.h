@@ -128,12 +128,18 @@ int viss_plan_set_samples(viss_plan *plan, int64_t K, const double *uvw, const d
  *   V_k = sum_j sky_j vis_kj exp(-2 pi i (u_k . s_j + off_k)),  k < K
  * sky: J FP32; V: K complex64.  Split precision by default (FP64 phase and
  * turn reduction, FP32 sincos, compensated FP32 sums, FP64 cross-block sum);
- * VISS_FP64 selects the plain FP64 path. */
+ * VISS_FP64 selects the plain FP64 path.  Asynchronous: VISS_OK means the
+ * work was launched.  A bounded device-side wait that gave up inside the
+ * kernel (V then incomplete) is reported only by the next
+ * viss_plan_last_stats / viss_plan_last_counts on this plan, which return
+ * VISS_ERR_TIMEOUT; callers that need the guarantee check it after the call. */
 int viss_forward(viss_plan *plan, const float *sky, float *V, int flags, void *stream);
 
 /* Imaging adjoint, replaces computeC (vissgen3d_blockage.cu:167-192):
  *   image_j = scale * sum_k Re(coef_k exp(+2 pi i (u_k . s_j + off_k))) vis_kj
- * coef: K complex64 (the weighted visibilities w_k V_k); image: J FP32. */
+ * coef: K complex64 (the weighted visibilities w_k V_k); image: J FP32.
+ * Asynchronous; a timed-out wait is reported as for viss_forward, only
+ * through viss_plan_last_stats / viss_plan_last_counts. */
 int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, int flags,
                  void *stream);
 
@@ -194,7 +200,9 @@ int viss_adjoint_formation(viss_plan *plan, const float *coef, float *image, flo
  * block's bounded waits give up (about 1 s each, no fault, no trap), the
  * kernel ends, and viss_plan_last_stats / viss_plan_last_counts then return
  * VISS_ERR_TIMEOUT; the plan and the context stay usable.  The results of
- * that one call are incomplete.  No counterpart in the reference. */
+ * that one call are incomplete.  With plan == NULL the hook arms the next
+ * viss_forward_noalloc call instead (process-wide), which then returns
+ * VISS_ERR_TIMEOUT itself.  No counterpart in the reference. */
 int viss_plan_debug_drop_copy(viss_plan *plan, int tile);
 
 /* Sets the launch shapes directly (indices 0..3 each). */
@@ -220,8 +228,12 @@ int viss_plan_last_stats(viss_plan *plan, int64_t *evaluated, int64_t *mixed, in
  * Limits: J <= 65536 pixels, K <= 32768 samples, G <= 98304 occulter rows
  * (else VISS_ERR_ARG).  The
  * first call on a device looks up the array's address (cudaGetSymbolAddress)
- * -- make it before any stream capture.  Calls share the array: calls that
- * overlap on the GPU race.  Each call synchronises `stream` once. */
+ * -- make it before any stream capture -- and keeps it for the life of the
+ * process, so the entry point must not be used across a cudaDeviceReset.
+ * Calls share the array: calls that overlap on the GPU race.  Each call
+ * synchronises `stream` twice (the phase-bound check before the kernel, the
+ * kernel's error word after it) and returns VISS_ERR_TIMEOUT, with V
+ * incomplete, if a bounded device-side wait gave up. */
 int viss_forward_noalloc(int64_t J, const double *lmn, const float *sky, int64_t K,
                          const double *uvw, const double *off, const int32_t *refs, int64_t G,
                          const double *occ, float *V, void *stream);

@@ -5,9 +5,11 @@
 # Only this variant is built: its kernels stay in bounds on valid inputs, while
 # the blockage variants' calculateDcf reads R[nr], mb[nr] one past the end
 # (vissgen3d_blockage.cu:138) and pix2ang.cu reads jrll[12] / pix2x[1024].
+# The reference sources are read from $REF, by default a "reference" folder
+# beside the repository.
 set -euo pipefail
-REF=${REF:-/root/reference}
 HERE="$(cd "$(dirname "$0")" && pwd)"
+REF=${REF:-$(cd "$HERE/../.." && pwd)/reference}
 OUT="$HERE/_ref"
 [ -d "$REF" ] || { echo "reference sources not found at $REF" >&2; exit 0; }
 mkdir -p "$OUT"

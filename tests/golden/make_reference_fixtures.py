@@ -8,7 +8,12 @@ reference is CUDA-only -- and keeps its inputs, its output C1day1M.txt and
 its stdout (which prints Viss[0..2], the forward visibilities before the
 w-rotation).
 
-    python tests/golden/make_reference_fixtures.py --out DIR [--ref PATH]
+    python tests/golden/make_reference_fixtures.py --out DIR [--ref PATH] [--case limb]
+
+--case golden (default) writes the case of refcase.make_case (every pixel at
+least 1e-4 from every occultation cone); --case limb the case of
+refcase.make_limb_case (ten bright probe pixels placed 3e-8 to 2e-6 from one
+satellite's cone each), also listing the probes in probes.json.
 """
 import argparse
 import os
@@ -29,10 +34,16 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--ref", default=os.path.join(ROOT, "oracle", "_ref", "vissgen3d_noblockage_10m"))
+    ap.add_argument("--case", choices=["golden", "limb"], default="golden")
     args = ap.parse_args()
-    case = refcase.make_case()
+    case = refcase.make_case() if args.case == "golden" else refcase.make_limb_case()
     with tempfile.TemporaryDirectory() as tmp:
         refcase.write_inputs(case, tmp, variant_10m=True)
+        if "probes" in case:
+            import json
+            with open(os.path.join(tmp, "probes.json"), "w") as f:
+                json.dump({"probe_pixels": [int(x) for x in case["probes"]],
+                           "targets": [float(x) for x in refcase.LIMB_TARGETS]}, f)
         os.makedirs(os.path.join(tmp, "3dnoblockage10M"))
         r = subprocess.run([args.ref], cwd=tmp, capture_output=True, text=True, timeout=600)
         with open(os.path.join(tmp, "reference_stdout.txt"), "w") as f:

@@ -74,6 +74,72 @@ def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10,
     return dict(theta=theta, phi=phi, B=B, uvw=uvw, xyza=xyza, xyzb=xyzb, bll=bll2)
 
 
+def _dir_to_theta_phi(s):
+    """HEALPix-style (theta, phi) whose (l, m, n) = (sin t cos p, -sin t sin p,
+    cos t) is the unit vector s (the convention of vissgen3d_blockage.cu:53-74)."""
+    th = math.acos(max(-1.0, min(1.0, float(s[2]))))
+    ph = math.atan2(-float(s[1]), float(s[0])) % (2 * math.pi)
+    return th, ph
+
+
+LIMB_TARGETS = (-2e-6, -6e-7, -2e-7, -6e-8, 0.0, 0.0, 6e-8, 2e-7, 6e-7, 2e-6)
+
+
+def make_limb_case(seed: int = 7, targets=LIMB_TARGETS, probe_sky: float = 40.0):
+    """The small case of make_case (every HEALPix pixel >= 1e-4 from every
+    occultation cone), with len(targets) pixels moved onto the cone of one
+    (snapshot, satellite) each: their FP64 predicate margin
+    s.P/|P| - cos(phi) is the target (as realised after the FP32 rounding of
+    the text inputs), and they stay >= 2e-5 from every other satellite's cone.
+    For such probes the reference's FP32 acosf predicate
+    (vissgen3d_blockage.cu:88-94) and the FP64 dot product may disagree.
+    Every probe is seen by another satellite of its snapshot, so its bit
+    shows in the reference's forward visibilities and hence in its image."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from oracle import oracle as O
+
+    case = make_case(seed=seed)
+    n = case["uvw"].shape[0] // 2
+    npix = case["B"].size
+    thr = O.cone_threshold(np.float32(1737.1e3), np.float32(300e3))
+    # the distinct satellite positions (snapshot-major), as the rows hold them
+    P = np.concatenate([case["xyza"][:n], case["xyzb"][:n]]).astype(np.float64)
+    Pu, first = np.unique(P, axis=0, return_index=True)
+    Pu = P[np.sort(first)]
+    q = Pu / np.linalg.norm(Pu, axis=1, keepdims=True)
+    rng = np.random.default_rng(seed + 100)
+    theta, phi, B = case["theta"].copy(), case["phi"].copy(), case["B"].copy()
+    slots = np.linspace(3, npix - 5, len(targets)).astype(int)
+    owners = rng.choice(len(Pu), len(targets), replace=False)
+    for slot, g, target in zip(slots, owners, targets):
+        qg = q[g]
+        # rows (a, b) of this satellite: the partners that must see the probe
+        partners = [i for i in range(len(Pu)) if i != g and np.linalg.norm(Pu[i] - Pu[g]) < 5e3]
+        for _attempt in range(20000):
+            w = rng.standard_normal(3)
+            w -= (w @ qg) * qg
+            w /= np.linalg.norm(w)
+            c = thr + target
+            s = c * qg + math.sqrt(1.0 - c * c) * w
+            th, ph = _dir_to_theta_phi(s)
+            th32, ph32 = np.float32(th), np.float32(ph)
+            lmn, _ = O.sky_pre_f32(np.array([th32]), np.array([ph32]), np.array([1.0], np.float32),
+                                   np.float32(1.0))
+            d = lmn[0] @ q.T - thr
+            others = np.delete(np.abs(d), g)
+            if (abs(d[g] - target) <= 1.5e-7 and others.min() > 2e-5
+                    and any(d[i] > 2e-5 for i in partners)):
+                theta[slot], phi[slot] = th32, ph32
+                B[slot] = np.float32(probe_sky)
+                break
+        else:
+            raise RuntimeError("no probe direction found")
+    case = dict(case, theta=theta, phi=phi, B=B)
+    case["probes"] = slots
+    return case
+
+
 def write_inputs(case, root: str, variant_10m: bool = True, day: int = 1):
     """The reference's input files under root (earth_10Mhz/ or earth_1Mhz/),
     the rows as day `day`."""
@@ -145,3 +211,97 @@ def oracle_vissgen(case, blockage: bool, frequency: float = 1e7, dcf_shift: bool
     C = O.adjoint(uvw, wt.astype(np.float64) * V, lmn, refs if blockage else None,
                   occ if blockage else None)
     return V0, C
+
+
+# ------------------------------------------------- limb: the reference's bits
+def satellite_table(case):
+    """Distinct satellite positions of the day's unique rows (FP64 from the
+    FP32 text), each row's two satellites as indices into them, and the
+    unit directions q = P/|P| of the reference's cone test."""
+    n = case["uvw"].shape[0] // 2
+    P = np.concatenate([case["xyza"][:n], case["xyzb"][:n]]).astype(np.float64)
+    Pu, inv = np.unique(P, axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    q = Pu / np.linalg.norm(Pu, axis=1, keepdims=True)
+    return Pu, q, inv[:n], inv[n:]
+
+
+def satellite_margins(case):
+    """(lmn, margin) with margin[j, g] = s_j . q_g - cos(phi): the FP64
+    predicate's distance from the reference's cone (visible iff >= 0) for
+    every pixel j and distinct satellite g."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from oracle import oracle as O
+    npix = case["B"].size
+    lmn, _ = O.sky_pre_f32(case["theta"], case["phi"], case["B"], np.float32(4 * math.pi / npix))
+    _Pu, q, _a, _b = satellite_table(case)
+    thr = O.cone_threshold(np.float32(1737.1e3), np.float32(300e3))
+    d = np.stack([O.dots(lmn, np.append(qg, 0.0)) for qg in q], axis=1) - thr
+    return lmn, d
+
+
+def vissgen_with_visibility(case, vis, frequency: float = 1e7):
+    """The noblockage program's day (vissgen3d_noblockage.cu:195-563) in FP64
+    for an explicit per-satellite visibility vis[j, g] (pixel j seen from
+    distinct satellite g): the forward's row mask is vis[:, a_i] & vis[:, b_i]
+    (:88-94), the imaging adjoint is unmasked (:167-182).  Returns (V of the
+    unique rows before the w-rotation, Re C per pixel)."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from oracle import oracle as O
+    npix = case["B"].size
+    s = np.float32(4 * math.pi / npix)
+    lmn, Bs = O.sky_pre_f32(case["theta"], case["phi"], case["B"], s)
+    uvw = case["uvw"].astype(np.float64)
+    n = uvw.shape[0]
+    amount = n // 2
+    w = uvw[:, 2]
+    _Pu, _q, a, b = satellite_table(case)
+    M = (vis[:, a] & vis[:, b]).T                                    # (amount, npix)
+    ph = uvw[:amount] @ lmn.T - w[:amount, None]
+    V = np.zeros(n, np.complex128)
+    V[:amount] = ((Bs.astype(np.float64)[None, :] * M) * np.exp(-2j * np.pi * ph)).sum(axis=1)
+    V[amount:] = np.conj(V[:amount])
+    V0 = V[:amount].copy()
+    lam = np.float32(3e8 / np.float32(frequency))
+    nr = int(np.ceil(np.float32(100e3) / lam * np.float32(2)))
+    gs, _counts, dcf = O.dcf(case["bll"], nr, 1)
+    V = O.wrot(w, V)
+    dg = O.gamma_dg(case["uvw"][:, 2], case["bll"][:n])
+    wt = O.weights(gs[:n], dg, dcf, nr)
+    C = np.real(((wt.astype(np.float64) * V)[:, None] * np.exp(2j * np.pi * (uvw @ lmn.T))).sum(axis=0))
+    return V0, C
+
+
+def infer_limb_bits(case, C_ref, band: float = 5e-6):
+    """The reference's visibility bits for the (pixel, satellite) pairs within
+    `band` of the cone, recovered from its image C_ref: the image is linear
+    in each such bit (the bit only gates that pixel's term in the rows of
+    that satellite), so every combination is evaluated and the one whose
+    image matches C_ref best is taken.  Every pair outside the band is the
+    FP64 predicate's.  Returns (pairs (j, g), margins, reference bits, FP64
+    bits, residual of the best combination, of the second best, the image
+    of each single-bit flip)."""
+    lmn, d = satellite_margins(case)
+    vis = d >= 0.0
+    pairs = [tuple(x) for x in np.argwhere(np.abs(d) <= band)]
+    m = len(pairs)
+    base = vis.copy()
+    for j, g in pairs:
+        base[j, g] = False
+    _, C0 = vissgen_with_visibility(case, base)
+    dC = []
+    for j, g in pairs:
+        v = base.copy()
+        v[j, g] = True
+        dC.append(vissgen_with_visibility(case, v)[1] - C0)
+    dC = np.array(dC).reshape(m, -1)
+    combos = ((np.arange(2 ** m)[:, None] >> np.arange(m)[None, :]) & 1).astype(np.float64)
+    images = C0[None, :] + combos @ dC
+    res = np.linalg.norm(images - C_ref[None, :], axis=1) / np.linalg.norm(C_ref)
+    order = np.argsort(res)
+    best = combos[order[0]].astype(bool)
+    ours = np.array([vis[j, g] for j, g in pairs], dtype=bool)
+    margins = np.array([d[j, g] for j, g in pairs])
+    return pairs, margins, best, ours, float(res[order[0]]), float(res[order[1]]) if m else np.inf, dC

@@ -49,3 +49,51 @@ def test_oracle_reproduces_reference_forward(oracle):
     Vref = reference_viss()
     assert Vref.size == 3
     np.testing.assert_allclose(V0[:3], Vref, rtol=2e-5, atol=2e-5 * np.abs(Vref).max())
+
+
+# ------------------------------------------------------------------ the limb
+LIMB = os.path.join(HERE, "golden", "ref_noblockage_10m_limb")
+LIMB_BAND = 5e-6      # |s.q - cos(phi)| within which the FP32 and FP64 predicates may differ
+
+
+def limb_reference_bits():
+    """The reference's own visibility bits at the limb probes, recovered from
+    its image (refcase.infer_limb_bits), with our FP64 predicate's bits."""
+    case = refcase.read_inputs(LIMB)
+    Cref = np.loadtxt(os.path.join(LIMB, "3dnoblockage10M", "C1day1M.txt"))
+    return case, Cref, refcase.infer_limb_bits(case, Cref, band=LIMB_BAND)
+
+
+def test_limb_fixture_inputs_are_the_generator_case():
+    case = refcase.read_inputs(LIMB)
+    gen = refcase.make_limb_case()
+    for k in ("theta", "phi", "B", "uvw", "xyza", "xyzb", "bll"):
+        np.testing.assert_array_equal(case[k], gen[k])
+
+
+def test_limb_reference_bits_are_determined(oracle):
+    """The reference program's image fixes its mask bit at every probe: one
+    combination reproduces it to the text's precision, the next best is at
+    least a hundred times worse.  Every (pixel, satellite) pair outside the band
+    takes the FP64 predicate's bit (any other bit would leave a residual of
+    ~1e-4 or more, far above the one accepted here)."""
+    case, Cref, (pairs, margins, ref_bits, our_bits, r_best, r_next, dC) = limb_reference_bits()
+    assert len(pairs) == len(refcase.LIMB_TARGETS)
+    assert np.abs(margins).max() <= LIMB_BAND
+    assert r_best <= 2e-5, r_best
+    assert r_next >= 100 * r_best, (r_best, r_next)
+    # every single flip moves the image far more than the accepted residual
+    assert (np.linalg.norm(dC, axis=1) / np.linalg.norm(Cref)).min() > 100 * r_best
+
+
+def test_limb_bits_agree_outside_the_fp32_error_band(oracle):
+    """Where the two predicates may disagree: the reference tests acosf(s.P/|P|)
+    <= phi in FP32 (vissgen3d_blockage.cu:88-94) with (l, m, n) from FP32
+    sinf/cosf of its FP32 angle edits (:53-74); this repository tests
+    s.P/|P| >= cos(phi) in FP64.  Their FP32 rounding moves the reference's
+    boundary by a few 1e-7 in the cosine, so a bit may differ only within that
+    distance of the cone: the probes at |margin| >= 5e-7 must agree."""
+    case, Cref, (pairs, margins, ref_bits, our_bits, r_best, r_next, dC) = limb_reference_bits()
+    far = np.abs(margins) >= 5e-7
+    assert far.sum() >= 4
+    np.testing.assert_array_equal(ref_bits[far], our_bits[far])

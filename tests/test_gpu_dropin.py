@@ -133,3 +133,29 @@ def test_malformed_inputs_end_with_a_message(tmp_path):
     os.makedirs(tmp_path / "3dblockage10M", exist_ok=True)
     r = call()
     assert r.returncode != 0 and "fewer rows than uvw" in r.stderr
+
+
+LIMB = os.path.join(ROOT, "tests", "golden", "ref_noblockage_10m_limb")
+
+
+def test_noblockage_10m_at_the_limb_differs_from_the_reference_only_by_its_fp32_bits(tmp_path, oracle):
+    """The limb fixture: ten bright probe pixels 3e-8 to 2e-6 (in the cosine)
+    from one satellite's occultation cone each, run through the reference's
+    own vissgen3d_noblockage_10m.  Its mask bits there are recovered from its
+    image (refcase.infer_limb_bits).  The drop-in applies the FP64 predicate:
+    its image equals the oracle's with the FP64 bits, and differs from the
+    reference's image by exactly the effect of the probes whose bits the two
+    predicates set differently (2e-5 of the largest value, the text's
+    precision)."""
+    case = refcase.read_inputs(LIMB)
+    refcase.write_inputs(case, str(tmp_path), variant_10m=True)
+    os.makedirs(tmp_path / "3dnoblockage10M")
+    run("vissgen3d_noblockage_10m", tmp_path)
+    C = np.loadtxt(tmp_path / "3dnoblockage10M" / "C1day1M.txt")
+    Cref = np.loadtxt(os.path.join(LIMB, "3dnoblockage10M", "C1day1M.txt"))
+    pairs, margins, ref_bits, our_bits, r_best, _r_next, dC = refcase.infer_limb_bits(case, Cref)
+    _, Co = refcase.oracle_vissgen(case, blockage=False)
+    scale = np.abs(Co).max()
+    assert np.abs(C - Co).max() <= 2e-5 * scale, np.abs(C - Co).max()
+    flip = (our_bits.astype(float) - ref_bits.astype(float)) @ dC
+    assert np.abs(C - (Cref + flip)).max() <= 4e-5 * scale, np.abs(C - (Cref + flip)).max()

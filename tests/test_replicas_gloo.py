@@ -70,6 +70,42 @@ def test_two_rank_day_sum_matches_single_process():
         assert mx == [1.0, 10.0]
 
 
+def _bench_worker(rank, world, port, steps, out):
+    """The day-sum path of bench.py --gpus N: every step adds this rank's day
+    image into an FP64 sum (replicas.add_day_image, non-finite pixels as 0),
+    and the last step all-reduces the sums (replicas.sum_images).  CPU
+    tensors stand in for the device images."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from viss_optimize_3d_b200 import replicas
+        day = replicas.days_for_rank(world, rank, world)[0]
+        total = torch.zeros(48, dtype=torch.float64)
+        for i in range(steps):
+            img = _day_image(day).to(torch.float32)
+            replicas.add_day_image(total, img)
+            if i == steps - 1:
+                replicas.sum_images(total)
+        out[rank] = total.numpy().tolist()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_bench_day_sum():
+    world, steps = 2, 3
+    port = _free_port()
+    manager = mp.get_context("spawn").Manager()
+    out = manager.dict()
+    mp.start_processes(_bench_worker, args=(world, port, steps, out), nprocs=world, start_method="spawn")
+    ref = np.zeros(48)
+    for day in (1, 2):
+        img = torch.nan_to_num(_day_image(day).to(torch.float32).double(), nan=0.0).numpy()
+        ref += steps * img
+    for rank in range(world):
+        np.testing.assert_allclose(out[rank], ref, rtol=1e-12, atol=1e-12)
+
+
 def test_days_for_rank_validates():
     from viss_optimize_3d_b200 import replicas
     assert replicas.days_for_rank(450, 3, 8)[:3] == [4, 12, 20]

@@ -402,3 +402,17 @@ def scale_coef(wt, V: torch.Tensor) -> torch.Tensor:
     out = torch.empty_like(V)
     check(lib.viss_scale_coef(V.shape[0], _p(wt), _p(V), _p(out), _stream(V)), "viss_scale_coef")
     return out
+
+
+def accumulate_image(total: torch.Tensor, img: torch.Tensor) -> torch.Tensor:
+    """total += img in FP64 with non-finite pixels counted as 0, on the device
+    (viss_accumulate_image): the day sum the reference's notebooks form on the
+    host (healpix3d_blockage.ipynb:103-116)."""
+    if total.dtype != torch.float64 or not total.is_contiguous() or not total.is_cuda:
+        raise ValueError("total must be a contiguous float64 CUDA tensor")
+    img = _cuda(img, torch.float32, total.device)
+    if img.numel() != total.numel():
+        raise ValueError("img and total must hold the same number of pixels")
+    check(lib.viss_accumulate_image(total.numel(), _p(img), _p(total), _stream(total)),
+          "viss_accumulate_image")
+    return total

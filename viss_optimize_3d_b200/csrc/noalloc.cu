@@ -19,8 +19,13 @@
 //     make that first call before any stream capture;
 //   - all calls share the one array, so calls that overlap on the GPU (two
 //     streams, two host threads) race and corrupt each other's results;
-//   - each call synchronises its stream once (it reads back the |u.s| bound
-//     that decides whether the split-precision phase is valid).
+//   - each call synchronises its stream twice: once to read back the |u.s|
+//     bound that decides whether the split-precision phase is valid, and once
+//     at the end to read the kernel's error word, so that a bounded staging
+//     wait that gave up is returned by this call as VISS_ERR_TIMEOUT;
+//   - the array's address is cached per device for the life of the process;
+//     after cudaDeviceReset (which unloads the module) the cached address is
+//     stale, so this entry point must not be used across a device reset.
 // Pixels are processed in the caller's order (no locality sort: sorting
 // needs temporary storage), so tiles of a non-NESTED input are less compact
 // and more of them take the per-term occultation test; results are the same.
@@ -43,6 +48,7 @@ cudaError_t launch_tile_cones(long long ntiles, const double4 *pix, float4 *cone
                               cudaStream_t st);
 cudaError_t launch_occ32(long long G, const double4 *occ, float4 *out, cudaStream_t st);
 int record_error(int status, const std::string &msg);
+int take_noalloc_drop_tile();
 }  // namespace viss
 
 namespace {
@@ -212,11 +218,22 @@ extern "C" int viss_forward_noalloc(int64_t J, const double *lmn, const float *s
   fp.channels = 1;
   fp.Kc = K;
   fp.pix_stride = Jpad;
-  fp.drop_tile = -1;
+  // test hook: viss_plan_debug_drop_copy(NULL, tile) arms the next call
+  fp.drop_tile = viss::take_noalloc_drop_tile();
   if ((e = viss::launch_forward(fp, shape, real_chunks, refs != nullptr, false, st)) != cudaSuccess)
     return na_cuda(e, "forward kernel");
   if ((e = viss::launch_reduce_fwd(K, real_chunks, part, reinterpret_cast<float2 *>(V), 0, st)) !=
       cudaSuccess)
     return na_cuda(e, "reduce");
+  // the kernel's error word: a bounded staging wait that gave up leaves V
+  // incomplete, and the caller learns it here rather than never
+  unsigned long long err = 0;
+  if ((e = cudaMemcpyAsync(&err, words + 1, sizeof(err), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return na_cuda(e, "error word");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return na_cuda(e, "sync");
+  if (err & viss::kErrTimeout)
+    return viss::record_error(VISS_ERR_TIMEOUT,
+                              "viss_forward_noalloc: a bounded shared-memory staging wait gave up; "
+                              "V is incomplete");
   return VISS_OK;
 }

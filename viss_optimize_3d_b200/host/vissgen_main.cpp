@@ -186,6 +186,7 @@ void run_day(int p, const Options &opt, const SkyInputs &sky, int nr, double thr
       VCALL(viss_plan_set_pixels(fplan, npix, d_lmn, nullptr));
       VCALL(viss_plan_set_samples(fplan, amount, d_uvw, d_off, d_refs, 2 * n, d_occ, nullptr));
       VCALL(viss_forward(fplan, d_Bs, d_V, flags, nullptr));
+      VCALL(viss_plan_last_counts(fplan, nullptr, nullptr));   // a bounded wait that gave up
       VCALL(viss_conj_mirror(amount, d_V, nullptr));
       VCALL(viss_plan_destroy(fplan));
     }
@@ -216,6 +217,7 @@ void run_day(int p, const Options &opt, const SkyInputs &sky, int nr, double thr
                                 VISS_VARIANT_BLOCKAGE ? 2 * n : 0, VISS_VARIANT_BLOCKAGE ? d_occ : nullptr,
                                 nullptr));
     VCALL(viss_adjoint(iplan, d_coef, d_img, 1.0f, flags, nullptr));
+    VCALL(viss_plan_last_counts(iplan, nullptr, nullptr));
     VCALL(viss_plan_destroy(iplan));
     CUCALL(cudaMemcpy(image.data(), d_img, sizeof(float) * npix, cudaMemcpyDeviceToHost));
     std::cout << "Period " << p + 1 << " compute C success" << std::endl;

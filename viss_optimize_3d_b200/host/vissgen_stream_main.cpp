@@ -321,7 +321,11 @@ class DevicePipeline {
       vcall(viss_plan_set_samples(iplan_, m, uvw_.p, nullptr, o_.blockage ? refs_.p : nullptr,
                                   o_.blockage ? 2 * n : 0, o_.blockage ? occ_.p : nullptr, cs_),
             "viss_plan_set_samples");
+      // set_samples synchronised cs_, so the forward has finished: did any of
+      // its bounded waits give up?
+      if (amount > 0) vcall(viss_plan_last_counts(fplan_, nullptr, nullptr), "viss_forward");
       vcall(viss_adjoint(iplan_, coef_.p, img_.p, scale, flags, cs_), "viss_adjoint");
+      vcall(viss_plan_last_counts(iplan_, nullptr, nullptr), "viss_adjoint");
     } else {
       cucall(cudaMemsetAsync(img_.p, 0, sky_.npix * sizeof(float), cs_), "memset");
     }

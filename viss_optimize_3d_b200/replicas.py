@@ -45,6 +45,18 @@ def sum_images(image: torch.Tensor) -> torch.Tensor:
     return image
 
 
+def add_day_image(total: torch.Tensor, img: torch.Tensor) -> torch.Tensor:
+    """total += img (FP64), non-finite pixels counted as 0.  On a CUDA device
+    this is one viss_accumulate_image launch; CPU tensors (the gloo tests'
+    stand-ins for a rank's images) take the same arithmetic in torch."""
+    if total.is_cuda:
+        from . import api
+        return api.accumulate_image(total, img)
+    img = torch.nan_to_num(img.to(torch.float64), nan=0.0, posinf=0.0, neginf=0.0)
+    total += img
+    return total
+
+
 def accumulate_days(n_days: int, npix: int, image_of_day: Callable[[int], torch.Tensor],
                     device=None, first_day: int = 1, nan_to_zero: bool = True) -> torch.Tensor:
     """Sum of image_of_day(d) over all days d, each rank computing its own
@@ -53,8 +65,9 @@ def accumulate_days(n_days: int, npix: int, image_of_day: Callable[[int], torch.
     world = dist.get_world_size() if _group_ready() else 1
     total = torch.zeros(npix, dtype=torch.float64, device=device)
     for d in days_for_rank(n_days, rank, world, first_day):
-        img = image_of_day(d).to(device=total.device, dtype=torch.float64)
+        img = image_of_day(d).to(device=total.device)
         if nan_to_zero:
-            img = torch.nan_to_num(img, nan=0.0, posinf=0.0, neginf=0.0)
-        total += img
+            add_day_image(total, img)
+        else:
+            total += img.to(torch.float64)
     return sum_images(total)

@@ -71,6 +71,12 @@ CONFIGS = {
                          moon=True, earth=True),
     "c3_10mhz": ObsConfig("c3_10mhz", nside=256, n_sat=10, n_snap=8640, freqs_hz=(1e7,),
                           moon=True, earth=True),
+    # the reference's production operating point at 1 MHz: Nside 512 and one
+    # day of up to 4,000,000 rows (vissgen3d_blockage.cu:28), i.e. 2,000,160
+    # unique samples once the mirror rows are folded (45 baselines x 44,448
+    # snapshots), Moon + Earth
+    "prod_1mhz": ObsConfig("prod_1mhz", nside=512, n_sat=10, n_snap=44448, freqs_hz=(1e6,),
+                           moon=True, earth=True),
     # batched: 64 channels 1-10 MHz
     "c4": ObsConfig("c4", nside=128, n_sat=10, n_snap=2880,
                     freqs_hz=tuple(np.linspace(1e6, 1e7, 64)), moon=True, earth=True),
