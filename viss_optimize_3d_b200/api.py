@@ -194,7 +194,9 @@ class Plan:
     def forward(self, sky, fp64: bool = False, mask: bool = True, use_offset: bool = True,
                 out: torch.Tensor | None = None) -> torch.Tensor:
         """healpix_moonback_viss (vissgen3d_blockage.cu:76-102):
-        V_k = sum_j sky_j vis_kj exp(-2 pi i (u_k.s_j + off_k)), complex64."""
+        V_k = sum_j sky_j vis_kj exp(-2 pi i (u_k.s_j + off_k)), complex64.
+        Asynchronous; a bounded device-side wait that gave up inside the
+        kernel is raised by the next last_stats() / last_counts()."""
         sky = _cuda(sky, torch.float32, self.device)
         if sky.numel() != self.channels * self.J:
             raise ValueError(f"sky must hold {self.channels} x {self.J} values")
@@ -210,7 +212,8 @@ class Plan:
     def adjoint(self, coef, scale: float = 1.0, fp64: bool = False, mask: bool = True,
                 use_offset: bool = True, out: torch.Tensor | None = None) -> torch.Tensor:
         """computeC (vissgen3d_blockage.cu:167-192):
-        img_j = scale * sum_k Re(coef_k exp(+2 pi i (u_k.s_j + off_k))) vis_kj."""
+        img_j = scale * sum_k Re(coef_k exp(+2 pi i (u_k.s_j + off_k))) vis_kj.
+        Asynchronous, like forward (a timed-out wait surfaces in last_stats())."""
         coef = _cuda(coef, torch.complex64, self.device)
         if coef.shape != (self.K,):
             raise ValueError(f"coef must have shape ({self.K},)")
