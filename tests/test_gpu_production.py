@@ -101,3 +101,68 @@ def test_production_size_split_accuracy(prod, oracle):
     g.plan.last_stats()
     Co = oracle.adjoint(uvw, a.astype(np.complex128), lmn[js], obs.refs, occ)
     assert rel_l2(Cs, Co) <= TOL_SPLIT, rel_l2(Cs, Co)
+
+
+# ------------------------------------------- the 10 MHz production limits
+# The reference's 10 MHz operating point is HEALPix Nside 4096 (201,326,592
+# pixels, healpix3d_blockage_10Mhz.ipynb:29) and up to 40,000,000 rows a day
+# (vissgen3d_blockage_10m.cu:28), i.e. 2e7 unique samples.  One full pass is
+# 4e15 terms (about half an hour on one B200), so each axis is exercised at its
+# full length separately: all 201,326,592 pixels with 2,048 samples, and
+# 20,000,025 samples with Nside 64.  Both run the plan set-up, the largest
+# grids (196,608 adjoint CTAs; 19,532 forward sample blocks) and the culling,
+# and check the integer visible-count identity (zero baselines, unit sky)
+# against viss_mask_bits.
+
+def _counts_identity(viss, lmn, refs, occ, dev, k_check, j_check):
+    K, J = refs.shape[0], lmn.shape[0]
+    plan0 = api.Plan(lmn, torch.zeros((K, 3), dtype=torch.float64, device=dev), None, refs, occ)
+    V = plan0.forward(torch.ones(J, dtype=torch.float32, device=dev))
+    plan0.last_stats()
+    img = plan0.adjoint(torch.ones(K, dtype=torch.complex64, device=dev))
+    plan0.last_stats()
+    # samples: popcounts of their full rows, 64 at a time
+    n_rows = []
+    for i in range(0, k_check.numel(), 64):
+        sel = k_check[i:i + 64]
+        n_rows.append(_popcount_rows(viss.mask_bits(lmn, refs[sel], occ).view(torch.uint8)))
+    rows = torch.cat(n_rows)
+    assert torch.equal(torch.round(V.real.double()[k_check]).long(), rows)
+    # pixels: popcounts over all samples of the checked pixels
+    lmn_sel = lmn[j_check].contiguous()
+    cols = torch.zeros(j_check.numel(), dtype=torch.int64, device=dev)
+    for k0 in range(0, K, 1 << 20):
+        cols += _popcount_cols(viss.mask_bits(lmn_sel, refs[k0:k0 + (1 << 20)], occ).view(torch.uint8),
+                               j_check.numel())
+    assert torch.equal(torch.round(img.double()[j_check]).long(), cols)
+    del plan0
+
+
+def test_10mhz_production_pixel_axis(viss, cuda_device):
+    import dataclasses
+    cfg = dataclasses.replace(synth.CONFIGS["c3_10mhz"], n_snap=8640)
+    obs = synth.make_observation(cfg)
+    # 2,048 samples spread over the orbit (every 190th): many occultation states
+    ks = np.arange(0, cfg.n_samples, 190)[:2048]
+    refs = torch.as_tensor(obs.refs[ks], device=cuda_device)
+    occ = pipeline.build_occulters(obs, cuda_device)
+    lmn = viss.pix2lmn(4096, "ring", device=cuda_device)
+    assert lmn.shape[0] == 201326592
+    rng = np.random.default_rng(41)
+    k_check = torch.as_tensor(np.sort(rng.choice(len(ks), 256, replace=False)), device=cuda_device)
+    j_check = torch.as_tensor(np.sort(rng.choice(lmn.shape[0], 8192, replace=False)), device=cuda_device)
+    _counts_identity(viss, lmn, refs, occ, cuda_device, k_check, j_check)
+
+
+def test_10mhz_production_sample_axis(viss, cuda_device):
+    import dataclasses
+    cfg = dataclasses.replace(synth.CONFIGS["c3_10mhz"], nside=64, n_snap=444445)
+    obs = synth.make_observation(cfg)
+    assert cfg.n_samples == 20000025
+    refs = torch.as_tensor(obs.refs, device=cuda_device)
+    occ = pipeline.build_occulters(obs, cuda_device)
+    lmn = viss.pix2lmn(64, "ring", device=cuda_device)
+    rng = np.random.default_rng(42)
+    k_check = torch.as_tensor(np.sort(rng.choice(cfg.n_samples, 4096, replace=False)), device=cuda_device)
+    j_check = torch.as_tensor(np.sort(rng.choice(lmn.shape[0], 1024, replace=False)), device=cuda_device)
+    _counts_identity(viss, lmn, refs, occ, cuda_device, k_check, j_check)

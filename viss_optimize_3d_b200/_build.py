@@ -87,8 +87,9 @@ HOST_PROGRAMS = {
     "vissgen3d_blockage_10m": ("vissgen_main.cpp", ["-DVISS_VARIANT_BLOCKAGE=1", "-DVISS_VARIANT_10M=1"]),
     "vissgen3d_noblockage": ("vissgen_main.cpp", ["-DVISS_VARIANT_BLOCKAGE=0", "-DVISS_VARIANT_10M=0"]),
     "vissgen3d_noblockage_10m": ("vissgen_main.cpp", ["-DVISS_VARIANT_BLOCKAGE=0", "-DVISS_VARIANT_10M=1"]),
-    # streaming day loop over binary day files (not a drop-in: new interface)
-    "vissgen_stream": ("vissgen_stream_main.cpp", []),
+    # streaming day loop over binary day files (not a drop-in: new interface);
+    # the per-GPU day sums are reduced with NCCL
+    "vissgen_stream": ("vissgen_stream_main.cpp", [], ["-lnccl"]),
 }
 
 
@@ -99,7 +100,7 @@ def build_host(force: bool = False, verbose: bool = False):
     os.makedirs(BIN, exist_ok=True)
     out = []
     common = [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith((".h", ".hpp"))]
-    for name, (src, defs) in HOST_PROGRAMS.items():
+    for name, (src, defs, *libs) in HOST_PROGRAMS.items():
         s = os.path.join(HOST, src)
         if not os.path.exists(s):
             continue
@@ -107,7 +108,8 @@ def build_host(force: bool = False, verbose: bool = False):
         if force or _newer(exe, [s, LIB, __file__] + common):
             cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-Wall", "-I", INCLUDE,
                    "-I", "/usr/local/cuda/include", *defs, s, "-o", exe, "-L", PKG, "-lviss",
-                   f"-Wl,-rpath,$ORIGIN/..", "-L/usr/local/cuda/lib64", "-lcudart", "-lpthread"]
+                   f"-Wl,-rpath,$ORIGIN/..", "-L/usr/local/cuda/lib64", "-lcudart", "-lpthread",
+                   *(libs[0] if libs else [])]
             _run(cmd, verbose)
         out.append(exe)
     return out

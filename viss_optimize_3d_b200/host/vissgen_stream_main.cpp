@@ -16,6 +16,9 @@
 //   * each day's image is summed on the device in FP64, non-finite pixels
 //     as 0 (viss_accumulate_image); per-day images are written by a writer
 //     thread from pinned memory when asked for.
+// After the last day the per-GPU FP64 sums are reduced onto GPU 0 by one NCCL
+// reduce (SUM), over NVLink where the GPUs have it; only that sum is copied
+// to the host.
 // The arithmetic per day is that of the drop-in executables
 // (host/vissgen_main.cpp): occultation rows of both satellites with the
 // reference's fixed cone, forward of the unique half with off = -w, conjugate
@@ -44,11 +47,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include <nccl.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include "dayfile.h"
@@ -167,7 +172,11 @@ class DevicePipeline {
   DevicePipeline(int dev, const Options &o, const Sky &sky, std::vector<int> days)
       : dev_(dev), o_(o), sky_(sky), days_(std::move(days)) {}
 
-  void run(std::vector<DayTiming> &timings, std::vector<double> &sum) {
+  // The day sum on this pipeline's device (FP64, npix), valid after run().
+  double *device_sum() const { return sum_.p; }
+  int device() const { return dev_; }
+
+  void run(std::vector<DayTiming> &timings) {
     cucall(cudaSetDevice(dev_), "cudaSetDevice");
     cucall(cudaStreamCreateWithFlags(&cs_, cudaStreamNonBlocking), "stream");
     cucall(cudaStreamCreateWithFlags(&xs_, cudaStreamNonBlocking), "stream");
@@ -234,8 +243,7 @@ class DevicePipeline {
     cv_.notify_all();
     if (writer.joinable()) writer.join();
     if (!write_error_.empty()) die(write_error_);
-    sum.assign(sky_.npix, 0.0);
-    cucall(cudaMemcpy(sum.data(), sum_.p, sky_.npix * sizeof(double), cudaMemcpyDeviceToHost), "sum");
+    cucall(cudaStreamSynchronize(cs_), "sync");
     vcall(viss_plan_destroy(fplan_), "viss_plan_destroy");
     vcall(viss_plan_destroy(iplan_), "viss_plan_destroy");
     for (Slot &s : slots_) {
@@ -482,6 +490,46 @@ bool read_day_image(const std::string &path, int64_t npix, std::vector<float> &i
   return ok;
 }
 
+void nccall(ncclResult_t r, const char *what) {
+  if (r != ncclSuccess) die(std::string(what) + ": " + ncclGetErrorString(r));
+}
+
+// The day sums of all pipelines' GPUs, reduced onto the first by one NCCL
+// reduce (FP64 SUM; a single GPU is a one-rank communicator), then added to
+// `total` on the host.
+void reduce_day_sums(const std::vector<std::unique_ptr<DevicePipeline>> &pipes, int64_t npix,
+                     std::vector<double> &total) {
+  const int n = static_cast<int>(pipes.size());
+  std::vector<int> devs(n);
+  for (int d = 0; d < n; ++d) devs[d] = pipes[d]->device();
+  std::vector<ncclComm_t> comms(n);
+  nccall(ncclCommInitAll(comms.data(), n, devs.data()), "ncclCommInitAll");
+  std::vector<cudaStream_t> st(n);
+  for (int d = 0; d < n; ++d) {
+    cucall(cudaSetDevice(devs[d]), "cudaSetDevice");
+    cucall(cudaStreamCreateWithFlags(&st[d], cudaStreamNonBlocking), "stream");
+  }
+  nccall(ncclGroupStart(), "ncclGroupStart");
+  for (int d = 0; d < n; ++d)
+    nccall(ncclReduce(pipes[d]->device_sum(), pipes[d]->device_sum(), static_cast<size_t>(npix),
+                      ncclFloat64, ncclSum, 0, comms[d], st[d]),
+           "ncclReduce");
+  nccall(ncclGroupEnd(), "ncclGroupEnd");
+  for (int d = 0; d < n; ++d) {
+    cucall(cudaSetDevice(devs[d]), "cudaSetDevice");
+    cucall(cudaStreamSynchronize(st[d]), "sync");
+  }
+  std::vector<double> sum(npix);
+  cucall(cudaSetDevice(devs[0]), "cudaSetDevice");
+  cucall(cudaMemcpy(sum.data(), pipes[0]->device_sum(), npix * sizeof(double), cudaMemcpyDeviceToHost),
+         "sum");
+  for (int64_t j = 0; j < npix; ++j) total[j] += sum[j];
+  for (int d = 0; d < n; ++d) {
+    ncclCommDestroy(comms[d]);
+    cudaStreamDestroy(st[d]);
+  }
+}
+
 int stream(const Options &o) {
   const auto t0 = std::chrono::steady_clock::now();
   const Sky sky = read_sky(o.sky);
@@ -505,14 +553,15 @@ int stream(const Options &o) {
   std::vector<std::vector<int>> mine(ndev);
   for (size_t k = 0; k < todo.size(); ++k) mine[k % ndev].push_back(todo[k]);  // :279
   std::vector<std::vector<DayTiming>> timings(ndev);
-  std::vector<std::vector<double>> sums(ndev, std::vector<double>(sky.npix, 0.0));
+  std::vector<std::unique_ptr<DevicePipeline>> pipes;
   std::vector<std::thread> threads;
-  for (int d = 0; d < ndev && !todo.empty(); ++d)
-    threads.emplace_back([&, d] { DevicePipeline(d, o, sky, mine[d]).run(timings[d], sums[d]); });
-  for (auto &t : threads) t.join();
-  // day sum: the resumed days, then the per-device FP64 sums in device order
-  for (int d = 0; d < ndev; ++d)
-    for (int64_t j = 0; j < sky.npix; ++j) total[j] += sums[d][j];
+  if (!todo.empty()) {
+    for (int d = 0; d < ndev; ++d) pipes.emplace_back(new DevicePipeline(d, o, sky, mine[d]));
+    for (int d = 0; d < ndev; ++d) threads.emplace_back([&, d] { pipes[d]->run(timings[d]); });
+    for (auto &t : threads) t.join();
+    reduce_day_sums(pipes, sky.npix, total);
+  }
+  // day sum: the resumed days plus the reduced device sums
   if (!o.sum_out.empty()) {
     const FileHeader h = viss_host::make_header("VISSIMG", 8, sky.npix, o.first_day, o.frequency, o.days);
     if (!viss_host::write_file(o.sum_out, h, total.data(), total.size() * sizeof(double)))
