@@ -115,26 +115,39 @@ def test_production_size_split_accuracy(prod, oracle):
 # against viss_mask_bits.
 
 def _counts_identity(viss, lmn, refs, occ, dev, k_check, j_check):
+    """The visible-count identity along both axes.  V and the image are FP32,
+    which holds integers exactly only below 2^24, so the unit sky (and the
+    unit coefficients) are split into slices of fewer than 2^24 pixels
+    (samples); each slice's count is then exact and the slices are summed."""
     K, J = refs.shape[0], lmn.shape[0]
+    lim = (1 << 24) - 1
     plan0 = api.Plan(lmn, torch.zeros((K, 3), dtype=torch.float64, device=dev), None, refs, occ)
-    V = plan0.forward(torch.ones(J, dtype=torch.float32, device=dev))
-    plan0.last_stats()
-    img = plan0.adjoint(torch.ones(K, dtype=torch.complex64, device=dev))
-    plan0.last_stats()
+    n_fwd = torch.zeros(K, dtype=torch.int64, device=dev)
+    for j0 in range(0, J, lim):
+        sky = torch.zeros(J, dtype=torch.float32, device=dev)
+        sky[j0:j0 + lim] = 1.0
+        n_fwd += torch.round(plan0.forward(sky).real.double()).long()
+        plan0.last_stats()
+    n_adj = torch.zeros(J, dtype=torch.int64, device=dev)
+    for k0 in range(0, K, lim):
+        coef = torch.zeros(K, dtype=torch.complex64, device=dev)
+        coef[k0:k0 + lim] = 1.0
+        n_adj += torch.round(plan0.adjoint(coef).double()).long()
+        plan0.last_stats()
     # samples: popcounts of their full rows, 64 at a time
     n_rows = []
     for i in range(0, k_check.numel(), 64):
         sel = k_check[i:i + 64]
         n_rows.append(_popcount_rows(viss.mask_bits(lmn, refs[sel], occ).view(torch.uint8)))
     rows = torch.cat(n_rows)
-    assert torch.equal(torch.round(V.real.double()[k_check]).long(), rows)
+    assert torch.equal(n_fwd[k_check], rows), int((n_fwd[k_check] != rows).sum())
     # pixels: popcounts over all samples of the checked pixels
     lmn_sel = lmn[j_check].contiguous()
     cols = torch.zeros(j_check.numel(), dtype=torch.int64, device=dev)
     for k0 in range(0, K, 1 << 20):
         cols += _popcount_cols(viss.mask_bits(lmn_sel, refs[k0:k0 + (1 << 20)], occ).view(torch.uint8),
                                j_check.numel())
-    assert torch.equal(torch.round(img.double()[j_check]).long(), cols)
+    assert torch.equal(n_adj[j_check], cols), int((n_adj[j_check] != cols).sum())
     del plan0
 
 
