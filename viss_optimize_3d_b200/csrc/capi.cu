@@ -36,7 +36,7 @@ cudaError_t launch_stage_pixels(long long, long long, const double *, const int 
 cudaError_t launch_occ32(long long, const double4 *, float4 *, cudaStream_t);
 cudaError_t launch_form_stage(long long, int, const double *, const double *, double4 *,
                               unsigned long long *, cudaStream_t);
-cudaError_t launch_form_stage_coef(long long, int, const float2 *, const double *, float4 *,
+cudaError_t launch_form_stage_coef(long long, int, const float2 *, const double *, float2 *,
                                    cudaStream_t);
 cudaError_t launch_form_reduce_fwd(long long, int, const double2 *, const double *, float2 *, int,
                                    cudaStream_t);
@@ -153,7 +153,7 @@ struct viss_plan {
   double4 *form_occ = nullptr;  size_t form_occ_cap = 0;   // [T*S satellites][T snapshots]
   float4 *form_occ32 = nullptr; size_t form_occ32_cap = 0;
   int form_sat = 0, form_snap = 0;
-  float4 *form_coef = nullptr;  size_t form_coef_cap = 0;
+  float2 *form_coef = nullptr;  size_t form_coef_cap = 0;
   // workspace + device status words
   void *part = nullptr;    size_t part_cap = 0;
   // [0] terms evaluated, [1] error flags, [2] terms evaluated in mixed tiles,
@@ -727,7 +727,7 @@ int viss_adjoint_formation(viss_plan *p, const float *coef, float *image, float 
   const cudaStream_t st = as_stream(stream);
   const long long T = p->form_T, B = viss::form_pairs(p->form_S);
   const int CB = viss::form_coef_stride(p->form_S);
-  if (int s = ensure(p->form_coef, p->form_coef_cap, sizeof(float4) * T * CB, "formation coefficients"))
+  if (int s = ensure(p->form_coef, p->form_coef_cap, sizeof(float2) * T * CB, "formation coefficients"))
     return s;
   const bool use_off = p->form_has_off && !(flags & VISS_NO_OFFSET);
   VISS_CUDA(viss::launch_form_stage_coef(T, p->form_S, reinterpret_cast<const float2 *>(coef),

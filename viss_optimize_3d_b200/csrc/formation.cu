@@ -87,16 +87,11 @@ __device__ __forceinline__ void classify(const float4 &cone, const float4 *row32
 // it take the exact per-pixel predicate.
 enum FormMode { kOpen = 0, kMixed = 1 };
 
-// One tile of kTilePix pixels for the warp's snapshot.  Per pixel: the S
-// exponentials F_b, then for each b the pair sums V_ab += G_a conj(F_b), a < b,
-// with G_a = I F_a.  Each pair sum is a packed (re, im) register pair updated
-// by two packed FMAs:
-//   (re, im) += (Gr, Gr) (c_b, s_b) + (-Gi, Gi) (s_b, c_b),   conj(F_b) = (c_b, s_b)
-// so G_a is kept as the two packed operands X1 = (Gr, Gr), X2 = (-Gi, Gi).
 template <int S, int MODE>
 __device__ __forceinline__ void form_fwd_tile(const double4 *tp, const double4 *U,
                                               const double4 *rows, unsigned hid, unsigned mix,
-                                              f32x2 (&acc)[form_pairs(S)]) {
+                                              float (&ar)[form_pairs(S)],
+                                              float (&ai)[form_pairs(S)]) {
   const int lane = threadIdx.x & 31;
 #pragma unroll 1
   for (int q = 0; q < kTilePix / 32; ++q) {
@@ -104,28 +99,28 @@ __device__ __forceinline__ void form_fwd_tile(const double4 *tp, const double4 *
     const double x = rec.x, y = rec.y, z = rec.z;
     float I = sky_bits(rec);
     if (MODE == kMixed && ((mix >> S) & 1u)) I = visible_row(rows[S], x, y, z) ? I : 0.f;
-    f32x2 X1[S - 1], X2[S - 1];
+    float Gr[S - 1], Gi[S - 1];
 #pragma unroll
     for (int b = 0; b < S; ++b) {
       float c, s;
-      sat_exp(U[b], x, y, z, c, s);          // F_b = m (c, -s)
+      sat_exp(U[b], x, y, z, c, s);
+      float Fr = c, Fi = -s;                 // F_b = m e^{-i theta}
       if (MODE != kOpen) {
         float m = ((hid >> b) & 1u) ? 0.f : 1.f;
         if (MODE == kMixed && ((mix >> b) & 1u)) m = visible_row(rows[b], x, y, z) ? m : 0.f;
-        c *= m;
-        s *= m;
+        Fr *= m;
+        Fi *= m;
       }
-      const f32x2 Y1 = pack2(c, s), Y2 = pack2(s, c);
+      const float cr = Fr, ci = -Fi;         // conj(F_b)
 #pragma unroll
       for (int a = 0; a < b; ++a) {
         const int pi = pair_index<S>(a, b);
-        fma2(acc[pi], X1[a], Y1);
-        fma2(acc[pi], X2[a], Y2);
+        ar[pi] = fmaf(Gr[a], cr, fmaf(-Gi[a], ci, ar[pi]));
+        ai[pi] = fmaf(Gr[a], ci, fmaf(Gi[a], cr, ai[pi]));
       }
       if (b < S - 1) {
-        const float gr = I * c, gi = -I * s;   // G_b = I F_b
-        X1[b] = pack2(gr, gr);
-        X2[b] = pack2(-gi, gi);
+        Gr[b] = I * Fr;
+        Gi[b] = I * Fi;
       }
     }
   }
@@ -184,17 +179,16 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
   }
   __syncthreads();
 
-  f32x2 acc[B];   // (re, im) of each pair, this lane's pixels since the last fold
+  float ar[B], ai[B];
 #pragma unroll
-  for (int k = 0; k < B; ++k) acc[k] = pack2(0.f, 0.f);
+  for (int k = 0; k < B; ++k) ar[k] = ai[k] = 0.f;
   double sr[(B + 31) / 32], si[(B + 31) / 32];
 #pragma unroll
   for (int k = 0; k < (B + 31) / 32; ++k) sr[k] = si[k] = 0.0;
   auto fold = [&]() {
 #pragma unroll
     for (int k = 0; k < B; ++k) {
-      float vr, vi;
-      unpack2(acc[k], vr, vi);
+      float vr = ar[k], vi = ai[k];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         vr += __shfl_xor_sync(0xffffffffu, vr, o);
@@ -204,7 +198,7 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
         sr[k >> 5] += vr;
         si[k >> 5] += vi;
       }
-      acc[k] = pack2(0.f, 0.f);
+      ar[k] = ai[k] = 0.f;
     }
   };
 
@@ -228,10 +222,10 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
     // a pair needs both satellites: skip the tile unless two see some of it
     if (tok && !snap_hidden && S - __popc(hid) >= 2) {
       if (mix | hid) {
-        form_fwd_tile<S, kMixed>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, acc);
+        form_fwd_tile<S, kMixed>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
         mixed_terms += static_cast<unsigned long long>(kTilePix) * B;
       } else {
-        form_fwd_tile<S, kOpen>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, acc);
+        form_fwd_tile<S, kOpen>(s_pix[stage], s_U[warp], s_row[warp], hid, mix, ar, ai);
       }
       evaluated += static_cast<unsigned long long>(kTilePix) * B;
     }
@@ -271,71 +265,72 @@ struct FormAdjStage {
   double4 snap[kFormSnapTile];
   float4 rows32[kFormSnapTile * S];
   float4 snap32[kFormSnapTile];
-  float4 coef[kFormSnapTile * form_coef_stride(S)];
+  float2 coef[kFormSnapTile * form_coef_stride(S)];
 };
 
-// Q[q] (one snapshot) for the lane's P pixels; cf is the snapshot's
-// coefficients (form_col0 column layout, (re, re, im, im) each), U its
-// satellite vectors.  For each b > 0, H_b = sum_{a<b} c'_ab K_a with
-// K_a = conj(F_a) = (c_a, s_a) is formed as two packed sums,
-//   A1 = sum c'.re (c_a, s_a),   A2 = sum c'.im (c_a, s_a)   (two packed FMAs a pair),
-// so H_b = (A1.re - A2.im, A1.im + A2.re), and Q += Re(H_b F_b) = Hr c_b + Hi s_b.
+// Q[q] (one snapshot) for the lane's P pixels; cf is the snapshot's column
+// layout of coefficients (form_col0), U its satellite vectors.
 template <int S, int P, int MODE>
-__device__ __forceinline__ void form_adj_snapshot(const double4 *U, const float4 *cf,
+__device__ __forceinline__ void form_adj_snapshot(const double4 *U, const float2 *cf,
                                                   const double4 *rows, unsigned hid, unsigned mix,
                                                   const double (&sx)[P], const double (&sy)[P],
                                                   const double (&sz)[P], float (&Q)[P]) {
-  f32x2 K[S - 1][P];
+  float Kr[S - 1][P], Ki[S - 1][P];
 #pragma unroll
   for (int q = 0; q < P; ++q) Q[q] = 0.f;
 #pragma unroll
   for (int b = 0; b < S; ++b) {
     const double4 Ub = U[b];
-    float Fc[P], Fs[P];   // F_b = (Fc, -Fs)
+    float Fr[P], Fi[P];
 #pragma unroll
     for (int q = 0; q < P; ++q) {
       float c, s;
       sat_exp(Ub, sx[q], sy[q], sz[q], c, s);
+      Fr[q] = c;
+      Fi[q] = -s;
       if (MODE != kOpen) {
         float m = ((hid >> b) & 1u) ? 0.f : 1.f;
         if (MODE == kMixed && ((mix >> b) & 1u)) m = visible_row(rows[b], sx[q], sy[q], sz[q]) ? m : 0.f;
-        c *= m;
-        s *= m;
+        Fr[q] *= m;
+        Fi[q] *= m;
       }
-      Fc[q] = c;
-      Fs[q] = s;
     }
     if (b > 0) {
-      f32x2 A1[P], A2[P];
+      float Hr[P], Hi[P];
 #pragma unroll
-      for (int q = 0; q < P; ++q) A1[q] = A2[q] = pack2(0.f, 0.f);
-      const f32x2 *col = reinterpret_cast<const f32x2 *>(cf + form_col0(b));
+      for (int q = 0; q < P; ++q) Hr[q] = Hi[q] = 0.f;
+      const float4 *col = reinterpret_cast<const float4 *>(cf + form_col0(b));
 #pragma unroll
-      for (int a = 0; a < b; ++a) {
-        const f32x2 cre = col[2 * a], cim = col[2 * a + 1];   // (re, re), (im, im)
+      for (int a2 = 0; a2 < b; a2 += 2) {
+        const float4 c2 = col[a2 / 2];  // coefficients of pairs (a2, b) and (a2 + 1, b)
 #pragma unroll
         for (int q = 0; q < P; ++q) {
-          fma2(A1[q], cre, K[a][q]);
-          fma2(A2[q], cim, K[a][q]);
+          Hr[q] = fmaf(c2.x, Kr[a2][q], fmaf(-c2.y, Ki[a2][q], Hr[q]));
+          Hi[q] = fmaf(c2.x, Ki[a2][q], fmaf(c2.y, Kr[a2][q], Hi[q]));
+        }
+        if (a2 + 1 < b) {
+#pragma unroll
+          for (int q = 0; q < P; ++q) {
+            Hr[q] = fmaf(c2.z, Kr[a2 + 1][q], fmaf(-c2.w, Ki[a2 + 1][q], Hr[q]));
+            Hi[q] = fmaf(c2.z, Ki[a2 + 1][q], fmaf(c2.w, Kr[a2 + 1][q], Hi[q]));
+          }
         }
       }
 #pragma unroll
-      for (int q = 0; q < P; ++q) {
-        float a1r, a1i, a2r, a2i;
-        unpack2(A1[q], a1r, a1i);
-        unpack2(A2[q], a2r, a2i);
-        Q[q] = fmaf(a1r - a2i, Fc[q], fmaf(a1i + a2r, Fs[q], Q[q]));
-      }
+      for (int q = 0; q < P; ++q) Q[q] = fmaf(Hr[q], Fr[q], fmaf(-Hi[q], Fi[q], Q[q]));
     }
     if (b < S - 1) {
 #pragma unroll
-      for (int q = 0; q < P; ++q) K[b][q] = pack2(Fc[q], Fs[q]);
+      for (int q = 0; q < P; ++q) {
+        Kr[b][q] = Fr[q];
+        Ki[b][q] = -Fi[q];
+      }
     }
   }
 }
 
 template <int S>
-__global__ void __launch_bounds__(kFormAdjNT, 2) k_form_adjoint(const FormParams p) {
+__global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams p) {
   constexpr int CB = form_coef_stride(S);
   constexpr int NW = kFormAdjNT / 32;
   constexpr int ST = 3;
@@ -366,12 +361,12 @@ __global__ void __launch_bounds__(kFormAdjNT, 2) k_form_adjoint(const FormParams
     const long long ts = s0 + static_cast<long long>(i) * kFormSnapTile;
     const int n = static_cast<int>(min(static_cast<long long>(kFormSnapTile), s1 - ts));
     FormAdjStage<S> &g = s_stage[stage];
-    uint32_t bytes = n * S * 32u + n * CB * 16u;
+    uint32_t bytes = n * S * 32u + n * CB * 8u;
     if (p.sat_rows) bytes += n * S * (32u + 16u);
     if (p.snap_rows) bytes += n * (32u + 16u);
     mbar_expect_tx(&s_full[stage], bytes);
     bulk_g2s(g.U, p.U + ts * S, n * S * 32u, &s_full[stage]);
-    bulk_g2s(g.coef, p.coef + ts * CB, n * CB * 16u, &s_full[stage]);
+    bulk_g2s(g.coef, p.coef + ts * CB, n * CB * 8u, &s_full[stage]);
     if (p.sat_rows) {
       bulk_g2s(g.rows, p.occ + ts * S, n * S * 32u, &s_full[stage]);
       bulk_g2s(g.rows32, p.occ32 + ts * S, n * S * 16u, &s_full[stage]);
@@ -534,10 +529,10 @@ __global__ void k_form_bound(long long n, const double *U, long long m, const do
   if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(b)));
 }
 
-// c'[t][form_col0(b) + a] = (re, re, im, im) of c[t B + pair(a, b)] e^{+2 pi i off}
-// (FP64 rotation).
+// c'[t][form_col0(b) + a] = c[t B + pair(a, b)] e^{+2 pi i off} (FP64
+// rotation), zero in the padding of each column.
 __global__ void k_form_stage_coef(long long T, int S, int CB, const float2 *coef, const double *off,
-                                  float4 *out) {
+                                  float2 *out) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= T * CB) return;
   const long long t = i / CB;
@@ -545,18 +540,21 @@ __global__ void k_form_stage_coef(long long T, int S, int CB, const float2 *coef
   int b = 1;
   while (b + 1 < S && form_col0(b + 1) <= r) ++b;
   const int a = r - form_col0(b);
+  if (a >= b) {
+    out[i] = make_float2(0.f, 0.f);
+    return;
+  }
   const long long k = t * form_pairs(S) + (a * S - a * (a + 1) / 2 + (b - a - 1));
   const float2 c = coef[k];
-  float re = c.x, im = c.y;
-  if (off) {
-    const double o = off[k];
-    double sn, cs;
-    sincospi(2.0 * (o - rint(o)), &sn, &cs);
-    const double dr = c.x, di = c.y;
-    re = static_cast<float>(dr * cs - di * sn);
-    im = static_cast<float>(dr * sn + di * cs);
+  if (!off) {
+    out[i] = c;
+    return;
   }
-  out[i] = make_float4(re, re, im, im);
+  const double o = off[k];
+  double sn, cs;
+  sincospi(2.0 * (o - rint(o)), &sn, &cs);
+  const double re = c.x, im = c.y;
+  out[i] = make_float2(static_cast<float>(re * cs - im * sn), static_cast<float>(re * sn + im * cs));
 }
 
 // V_k = e^{-2 pi i off_k} sum over chunks (FP64), optionally accumulated.
@@ -599,7 +597,7 @@ cudaError_t launch_form_stage(long long T, int S, const double *U, const double 
 }
 
 cudaError_t launch_form_stage_coef(long long T, int S, const float2 *coef, const double *off,
-                                   float4 *out, cudaStream_t st) {
+                                   float2 *out, cudaStream_t st) {
   const int CB = form_coef_stride(S);
   k_form_stage_coef<<<nblk(T * CB, 256), 256, 0, st>>>(T, S, CB, coef, off, out);
   return cudaGetLastError();

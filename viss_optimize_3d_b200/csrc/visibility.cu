@@ -169,10 +169,9 @@ __device__ __forceinline__ void sincos_turns_fp64(double t, double &sn, double &
   sincospi(2.0 * f, &sn, &cs);
 }
 
-// One forward term: sky I at phase t.  Split path: (re, im) += (I, -I) (cos, sin)
-// as one packed FMA, X = (I, -I) packed once per pixel; FP64 path: (dre, dim).
+// One forward term into (re, im): sky I at phase t.
 template <bool FP64>
-__device__ __forceinline__ void fwd_term(double t, float I, f32x2 X, f32x2 &acc, double &dre,
+__device__ __forceinline__ void fwd_term(double t, float I, float &re, float &im, double &dre,
                                          double &dim) {
   if (FP64) {
     double sn, cs;
@@ -182,7 +181,8 @@ __device__ __forceinline__ void fwd_term(double t, float I, f32x2 X, f32x2 &acc,
   } else {
     float sn, cs;
     sfu_sincos(turn_angle(t), sn, cs);
-    fma2(acc, X, pack2(cs, sn));
+    re = fmaf(I, cs, re);
+    im = fmaf(-I, sn, im);
   }
 }
 
@@ -198,8 +198,8 @@ constexpr int kSubPix = 32;
 template <int NROWS, bool FP64>
 __device__ __forceinline__ void fwd_span(const double4 *tp, double ux, double uy, double uz,
                                          double mk, double mk2, const double4 &q0,
-                                         const double4 &q1, const double4 &q2, f32x2 &acc,
-                                         double &dre, double &dim) {
+                                         const double4 &q1, const double4 &q2, float &re,
+                                         float &im, double &dre, double &dim) {
 #pragma unroll 2
   for (int j = 0; j < kSubPix; j += 2) {
     const double4 a = tp[j], b = tp[j + 1];
@@ -209,9 +209,9 @@ __device__ __forceinline__ void fwd_span(const double4 *tp, double ux, double uy
       Ib = visible_rows<NROWS>(q0, q1, q2, b.x, b.y, b.z) ? Ib : 0.f;
     }
     const double ta = fma(uz, a.z, fma(uy, a.y, fma(ux, a.x, mk)));
-    fwd_term<FP64>(ta, Ia, pack2(Ia, -Ia), acc, dre, dim);
+    fwd_term<FP64>(ta, Ia, re, im, dre, dim);
     const double tb = fma(uz, b.z, fma(uy, b.y, fma(ux, b.x, mk2)));
-    fwd_term<FP64>(tb, Ib, pack2(Ib, -Ib), acc, dre, dim);
+    fwd_term<FP64>(tb, Ib, re, im, dre, dim);
   }
 }
 
@@ -334,23 +334,22 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
     }
     const double4 *tp = s_pix[stage];
     if (mode != 0) {
-      f32x2 t_acc[R];   // split path: (re, im) over this tile
+      float t_re[R], t_im[R];
       double e_re[R], e_im[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) { t_acc[r] = pack2(0.f, 0.f); e_re[r] = e_im[r] = 0.0; }
+      for (int r = 0; r < R; ++r) { t_re[r] = t_im[r] = 0.f; e_re[r] = e_im[r] = 0.0; }
       if (mode == 2) {
         if ((tid & 31) == 0) evaluated += static_cast<unsigned long long>(nval_warp) * kTilePix;
         for (int j = 0; j < kTilePix; j += 2) {
           const double4 q0 = tp[j], q1 = tp[j + 1];
           const float I0 = sky_of(q0);
           const float I1 = FP64 ? sky_of(q1) : -sky_of(q1);
-          const f32x2 X0 = pack2(I0, -I0), X1 = pack2(I1, -I1);
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const double t0 = fma(uz[r], q0.z, fma(uy[r], q0.y, fma(ux[r], q0.x, mk[r])));
-            fwd_term<FP64>(t0, I0, X0, t_acc[r], e_re[r], e_im[r]);
+            fwd_term<FP64>(t0, I0, t_re[r], t_im[r], e_re[r], e_im[r]);
             const double t1 = fma(uz[r], q1.z, fma(uy[r], q1.y, fma(ux[r], q1.x, mk2[r])));
-            fwd_term<FP64>(t1, I1, X1, t_acc[r], e_re[r], e_im[r]);
+            fwd_term<FP64>(t1, I1, t_re[r], t_im[r], e_re[r], e_im[r]);
           }
         }
       } else {
@@ -388,13 +387,13 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
             if (sst == 0) continue;
             const double4 *sp = tp + b * kSubPix;
             if (wn == 0)
-              fwd_span<0, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_acc[r], e_re[r], e_im[r]);
+              fwd_span<0, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
             else if (wn == 1)
-              fwd_span<1, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_acc[r], e_re[r], e_im[r]);
+              fwd_span<1, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
             else if (wn == 2)
-              fwd_span<2, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_acc[r], e_re[r], e_im[r]);
+              fwd_span<2, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
             else
-              fwd_span<3, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_acc[r], e_re[r], e_im[r]);
+              fwd_span<3, FP64>(sp, ux[r], uy[r], uz[r], mk[r], mk2[r], q0, q1, q2, t_re[r], t_im[r], e_re[r], e_im[r]);
           }
         }
       }
@@ -406,10 +405,8 @@ __global__ void __launch_bounds__(NT, MINB) k_forward(const FwdParams p) {
         } else {
           float s0 = s_kahan[0][r][tid], c0 = s_kahan[1][r][tid];
           float s1 = s_kahan[2][r][tid], c1 = s_kahan[3][r][tid];
-          float t_re, t_im;
-          unpack2(t_acc[r], t_re, t_im);
-          kahan_add(s0, c0, t_re);
-          kahan_add(s1, c1, t_im);
+          kahan_add(s0, c0, t_re[r]);
+          kahan_add(s1, c1, t_im[r]);
           s_kahan[0][r][tid] = s0; s_kahan[1][r][tid] = c0;
           s_kahan[2][r][tid] = s1; s_kahan[3][r][tid] = c1;
         }
@@ -468,29 +465,27 @@ __global__ void k_reduce_fwd(long long K, int nchunk, const double2 *part, float
 // every term.  The P terms stay one branch-free block: splitting them by
 // sub-tile would serialise their DFMA -> MUFU latency chains, which costs more
 // than evaluating a hidden term.
-// Split path: acc[q] holds (sum a.re cos, sum -a.im sin) as a packed pair, one
-// packed FMA per term; Re(a e^{i x}) is the sum of its two halves.
 template <int P, int NROWS, bool FP64>
 __device__ __forceinline__ void adj_sample(const double4 &u, double m, const float2 &a,
                                            const double (&sx)[P], const double (&sy)[P],
                                            const double (&sz)[P], const double4 &q0,
                                            const double4 &q1, const double4 &q2, unsigned hid,
-                                           f32x2 (&acc)[P], double (&dacc)[P]) {
-  const f32x2 X = pack2(a.x, -a.y), zero = pack2(0.f, 0.f);
+                                           float (&acc)[P], double (&dacc)[P]) {
 #pragma unroll
   for (int q = 0; q < P; ++q) {
     const double t = fma(u.z, sz[q], fma(u.y, sy[q], fma(u.x, sx[q], m)));
     bool vis = ((hid >> q) & 1u) == 0;
     if (NROWS > 0) vis = vis & visible_rows<NROWS>(q0, q1, q2, sx[q], sy[q], sz[q]);
+    const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
     if (FP64) {
-      const float ar = vis ? a.x : 0.f, ai = vis ? a.y : 0.f;
       double sn, cs;
       sincos_turns_fp64(t, sn, cs);
       dacc[q] += fma(static_cast<double>(ar), cs, -static_cast<double>(ai) * sn);
     } else {
       float sn, cs;
       sfu_sincos(turn_angle(t), sn, cs);
-      fma2(acc[q], vis ? X : zero, pack2(cs, sn));
+      acc[q] = fmaf(ar, cs, acc[q]);
+      acc[q] = fmaf(-ai, sn, acc[q]);
     }
   }
 }
@@ -597,10 +592,10 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
     const float2 *cp = s_coef[buf];
     // plain FP32 sums over this staged tile (<= 128 samples per pixel), then
     // one Kahan fold into shared memory
-    f32x2 t_acc[P];
+    float t_acc[P];
     double e_acc[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) { t_acc[q] = pack2(0.f, 0.f); e_acc[q] = 0.0; }
+    for (int q = 0; q < P; ++q) { t_acc[q] = 0.f; e_acc[q] = 0.0; }
     for (int g = 0; g < n; g += 32) {
       // lane l classifies sample g+l against this warp's pixels; a sample
       // that is mixed on the warp's tile(s) is refined against the P
@@ -680,9 +675,7 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
         dacc[q] += e_acc[q];
       } else {
         float s = s_kahan[0][q][tid], c = s_kahan[1][q][tid];
-        float tc, ts;
-        unpack2(t_acc[q], tc, ts);
-        kahan_add(s, c, tc + ts);
+        kahan_add(s, c, t_acc[q]);
         s_kahan[0][q][tid] = s;
         s_kahan[1][q][tid] = c;
       }

@@ -59,12 +59,13 @@ constexpr int kFormAdjNT = 256;    // adjoint: threads per block
 constexpr int kFormSnapTile = 8;   // snapshots per adjoint staging tile
 constexpr int kFormFoldTiles = 32; // forward: pixel tiles between FP64 folds
 __host__ __device__ constexpr int form_pairs(int S) { return S * (S - 1) / 2; }
-// Adjoint coefficient layout per snapshot: one float4 (re, re, im, im) per
-// pair, column by column -- column b holds the pairs (a, b), a = 0..b-1, and
-// starts at form_col0(b) = b(b-1)/2 -- so that one 16-byte shared-memory read
-// gives both packed operands of the pair's two packed FMAs.
-__host__ __device__ constexpr int form_col0(int b) { return b * (b - 1) / 2; }
-__host__ __device__ constexpr int form_coef_stride(int S) { return form_pairs(S); }
+// Adjoint coefficient layout per snapshot: column b (pairs a < b, a = 0..b-1)
+// starts at form_col0(b) and is padded to an even length with zeros, so that
+// two coefficients load as one 16-byte shared-memory read.
+// Columns 1..b-1 hold b' entries each, rounded up to even:
+// sum = b(b-1)/2 + (odd b' in [1, b)) = b(b-1)/2 + floor(b/2).
+__host__ __device__ constexpr int form_col0(int b) { return b * (b - 1) / 2 + b / 2; }
+__host__ __device__ constexpr int form_coef_stride(int S) { return form_col0(S); }
 
 struct FormParams {
   const double4 *U;       // [T][S] satellite vectors in wavelengths (.w unused)
@@ -81,8 +82,8 @@ struct FormParams {
   int tiles_per_chunk;    // forward
   int snaps_per_chunk;    // adjoint, a multiple of kFormSnapTile
   int nchunk;             // forward: chunks; adjoint: chunks per channel
-  const float4 *coef;     // adjoint: [T][form_coef_stride(S)] coefficients, offsets applied,
-                          // (re, re, im, im) in the column layout of form_col0
+  const float2 *coef;     // adjoint: [T][form_coef_stride(S)] coefficients, offsets applied,
+                          // column layout of form_col0
   double2 *part_fwd;      // [chunk][T * B]
   double *part_adj;       // [channel][chunk][Jpad]
   unsigned long long *counter;

@@ -199,35 +199,6 @@ __device__ __forceinline__ void sfu_sincos(float a, float &s, float &c) {
   asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(a));
 }
 
-// ------------------------------------------------------ packed FP32 pairs
-// Two FP32 values in one 64-bit register pair, for sm_100's packed FP32
-// arithmetic (fma.rn.f32x2 and friends): one instruction issues two
-// independent round-to-nearest FMAs, so a complex multiply-accumulate
-// (4 FMAs) takes two issue slots instead of four.  Element 0 is the low word.
-typedef unsigned long long f32x2;
-
-__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
-  f32x2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-
-__device__ __forceinline__ void unpack2(f32x2 v, float &lo, float &hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-
-// d = a * b + d, elementwise, each element rounded once.
-__device__ __forceinline__ void fma2(f32x2 &d, f32x2 a, f32x2 b) {
-  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
-}
-
-// a * b, elementwise.
-__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
-  f32x2 r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-
 // Exact-op-order dot product used by the occultation predicate (the oracle
 // evaluates the same IEEE operations).
 __device__ __forceinline__ double dot_exact(double s0, double s1, double s2, const double4 &q) {
