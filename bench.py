@@ -104,6 +104,7 @@ def record_traffic(csv_path: str, workload: str, command: str):
     metrics log (dram__bytes_read.sum, dram__bytes_write.sum) into the traffic
     record, keyed by the current kernel sources' sha256."""
     import csv
+    import re
     per = {}
     with open(csv_path) as f:
         lines = [ln for ln in f if ln.startswith('"')]
@@ -114,11 +115,11 @@ def record_traffic(csv_path: str, workload: str, command: str):
             continue
         unit = row.get("Metric Unit", "byte")
         scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
-        for k in ("k_form_forward", "k_form_adjoint", "k_forward", "k_adjoint"):
-            if k + "<" in name or name.endswith(k):
-                per.setdefault(k, {}).setdefault(row.get("ID"), 0.0)
-                per[k][row.get("ID")] += float(val) * scale
-                break
+        m = re.search(r"\b(k_form_forward|k_form_adjoint|k_forward|k_adjoint)(_split)?<", name)
+        if m:
+            k = m.group(1)     # the split formation forward is recorded as k_form_forward
+            per.setdefault(k, {}).setdefault(row.get("ID"), 0.0)
+            per[k][row.get("ID")] += float(val) * scale
     try:
         with open(TRAFFIC_RECORD) as f:
             rec = json.load(f)

@@ -39,9 +39,12 @@ def test_traffic_record_roundtrip(bench, tmp_path):
     for mb in (90, 100, 101, 102):             # four forward launches, the last three are timed
         rows += [(fwd, "dram__bytes_read.sum", "Mbyte", f"{mb}"), (fwd, "dram__bytes_write.sum", "byte", "1,000")]
     rows += [(adj, "dram__bytes_read.sum", "Gbyte", "0.5"), (adj, "dram__bytes_write.sum", "Mbyte", "2")]
+    form = "void viss::k_form_forward_split<10>(viss::FormParams)"
+    rows += [(form, "dram__bytes_read.sum", "Mbyte", "33"), (form, "dram__bytes_write.sum", "byte", "0")]
     rec = bench.record_traffic(_csv(tmp_path, rows), "c3_10mhz", "ncu ...")
     assert rec["bytes_per_launch"]["c3_10mhz"]["k_forward"] == 101_001_000
     assert rec["bytes_per_launch"]["c3_10mhz"]["k_adjoint"] == 502_000_000
+    assert rec["bytes_per_launch"]["c3_10mhz"]["k_form_forward"] == 33_000_000
     v, src = bench.measured_traffic("c3_10mhz", "k_forward")
     assert v == 101_001_000 and "these kernel sources" in src
     assert bench.measured_traffic("c2", "k_forward")[0] is None

@@ -125,6 +125,17 @@ def test_device_day_sum(three_days):
     assert np.array_equal(total, host)
 
 
+def test_day_sum_through_the_nccl_reduce(three_days):
+    """The multi-GPU path of the day sum (one NCCL reduce of the per-GPU FP64
+    sums onto GPU 0), forced on one GPU as a one-rank communicator: the same
+    sum, bit for bit."""
+    root, cfg, _ = three_days
+    total = dayfile.read_image(root / "sum.vimg")[0]
+    run("vissgen_stream", "--sky", root / "bin" / "sky.vsky", "--days-dir", root / "bin", "--days", "3",
+        "--frequency", "1e6", "--blockage", "1", "--nccl-reduce", "--sum-out", root / "sum_nccl.vimg")
+    assert np.array_equal(dayfile.read_image(root / "sum_nccl.vimg")[0], total)
+
+
 def test_fold_mirrors_and_fp64(three_days):
     root, cfg, _ = three_days
     total = dayfile.read_image(root / "sum.vimg")[0]

@@ -18,7 +18,7 @@
 //     thread from pinned memory when asked for.
 // After the last day the per-GPU FP64 sums are reduced onto GPU 0 by one NCCL
 // reduce (SUM), over NVLink where the GPUs have it; only that sum is copied
-// to the host.
+// to the host (one GPU: a plain copy, or the NCCL path with --nccl-reduce).
 // The arithmetic per day is that of the drop-in executables
 // (host/vissgen_main.cpp): occultation rows of both satellites with the
 // reference's fixed cone, forward of the unique half with off = -w, conjugate
@@ -29,7 +29,7 @@
 //
 //   vissgen_stream --sky SKY.vsky --days-dir DIR [--first-day D] [--days N]
 //                  [--frequency HZ] [--blockage 0|1] [--fold-mirrors] [--fp64]
-//                  [--out-dir DIR [--resume]] [--sum-out FILE] [--devices N]
+//                  [--out-dir DIR [--resume]] [--sum-out FILE] [--devices N] [--nccl-reduce]
 // --resume skips the days whose image an earlier run already wrote to
 // --out-dir (a valid C{d}.vimg) and adds those images to the day sum instead,
 // so an interrupted run continues where it stopped.  Each day is one NVTX
@@ -69,6 +69,7 @@ struct Options {
   int first_day = 1, days = 1, max_devices = 1 << 20;
   double frequency = 1e6;
   bool blockage = true, fold = false, fp64 = false, resume = false;
+  bool nccl_reduce = false;   // --nccl-reduce: the NCCL reduce even on one GPU
   std::string convert_src, convert_dst, info;
   bool text_10m = false;
 };
@@ -495,13 +496,22 @@ void nccall(ncclResult_t r, const char *what) {
 }
 
 // The day sums of all pipelines' GPUs, reduced onto the first by one NCCL
-// reduce (FP64 SUM; a single GPU is a one-rank communicator), then added to
-// `total` on the host.
+// reduce (FP64 SUM), then added to `total` on the host.  With one GPU the
+// reduce is skipped (communicator set-up costs about a second) unless
+// `use_nccl` asks for it (a one-rank communicator; the tests use it).
 void reduce_day_sums(const std::vector<std::unique_ptr<DevicePipeline>> &pipes, int64_t npix,
-                     std::vector<double> &total) {
+                     std::vector<double> &total, bool use_nccl) {
   const int n = static_cast<int>(pipes.size());
   std::vector<int> devs(n);
   for (int d = 0; d < n; ++d) devs[d] = pipes[d]->device();
+  if (n == 1 && !use_nccl) {
+    std::vector<double> sum(npix);
+    cucall(cudaSetDevice(devs[0]), "cudaSetDevice");
+    cucall(cudaMemcpy(sum.data(), pipes[0]->device_sum(), npix * sizeof(double), cudaMemcpyDeviceToHost),
+           "sum");
+    for (int64_t j = 0; j < npix; ++j) total[j] += sum[j];
+    return;
+  }
   std::vector<ncclComm_t> comms(n);
   nccall(ncclCommInitAll(comms.data(), n, devs.data()), "ncclCommInitAll");
   std::vector<cudaStream_t> st(n);
@@ -559,7 +569,7 @@ int stream(const Options &o) {
     for (int d = 0; d < ndev; ++d) pipes.emplace_back(new DevicePipeline(d, o, sky, mine[d]));
     for (int d = 0; d < ndev; ++d) threads.emplace_back([&, d] { pipes[d]->run(timings[d]); });
     for (auto &t : threads) t.join();
-    reduce_day_sums(pipes, sky.npix, total);
+    reduce_day_sums(pipes, sky.npix, total, o.nccl_reduce);
   }
   // day sum: the resumed days plus the reduced device sums
   if (!o.sum_out.empty()) {
@@ -666,6 +676,7 @@ int main(int argc, char **argv) {
     else if (a == "--frequency") o.frequency = std::atof(val("--frequency").c_str());
     else if (a == "--blockage") o.blockage = std::atoi(val("--blockage").c_str()) != 0;
     else if (a == "--fold-mirrors") o.fold = true;
+    else if (a == "--nccl-reduce") o.nccl_reduce = true;
     else if (a == "--resume") o.resume = true;
     else if (a == "--fp64") o.fp64 = true;
     else if (a == "--out-dir") o.out_dir = val("--out-dir");
