@@ -81,9 +81,16 @@ def kernel_sources_sha() -> str:
     return h.hexdigest()
 
 
+FWD_INSTANCES = ["k_forward<256, 4, 2, {m}, 0>", "k_forward<256, 4, 3, {m}, 0>",
+                 "k_forward<256, 2, 3, {m}, 0>", "k_forward<256, 2, 4, {m}, 0>"]
+ADJ_INSTANCES = ["k_adjoint<128, 8, 4, {m}, 0>", "k_adjoint<128, 8, 5, {m}, 0>",
+                 "k_adjoint<128, 4, 5, {m}, 0>", "k_adjoint<128, 4, 6, {m}, 0>"]
+
+
 def measured_traffic(workload: str, kernel: str):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
-    of `kernel` on `workload` from an ncu capture recorded by
+    of the kernel instance `kernel` (e.g. "k_adjoint<128, 8, 4, 1, 0>", the
+    launch shape the run used) on `workload`, from an ncu capture recorded by
     `bench.py --record-traffic`, or None when no capture of the current
     kernel sources exists (a record of other sources is never reported)."""
     try:
@@ -99,7 +106,7 @@ def measured_traffic(workload: str, kernel: str):
     return v, f"ncu capture of these kernel sources (git {rec.get('git_commit', '?')}): {rec.get('command', '')}"
 
 
-def record_traffic(csv_path: str, workload: str, command: str):
+def record_traffic(csv_path: str, workload: str, command: str, commit: str = ""):
     """Write the DRAM traffic per launch of each kernel in an ncu --csv
     metrics log (dram__bytes_read.sum, dram__bytes_write.sum) into the traffic
     record, keyed by the current kernel sources' sha256."""
@@ -115,9 +122,9 @@ def record_traffic(csv_path: str, workload: str, command: str):
             continue
         unit = row.get("Metric Unit", "byte")
         scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
-        m = re.search(r"\b(k_form_forward|k_form_adjoint|k_forward|k_adjoint)(_split)?<", name)
+        m = re.search(r"\b((?:k_form_forward|k_form_adjoint|k_forward|k_adjoint)<[^>]*>)", name)
         if m:
-            k = m.group(1)     # the split formation forward is recorded as k_form_forward
+            k = m.group(1)     # the template instance, e.g. k_adjoint<128, 8, 4, 1, 0>
             per.setdefault(k, {}).setdefault(row.get("ID"), 0.0)
             per[k][row.get("ID")] += float(val) * scale
     try:
@@ -129,15 +136,13 @@ def record_traffic(csv_path: str, workload: str, command: str):
     if rec.get("kernel_sources_sha256") != sha:
         rec = {"kernel_sources_sha256": sha, "bytes_per_launch": {}}
     try:
-        rec["git_commit"] = subprocess.run(["git", "rev-parse", "--short", "HEAD"], cwd=ROOT,
-                                           capture_output=True, text=True).stdout.strip() or "?"
+        rec["git_commit"] = commit or subprocess.run(["git", "rev-parse", "--short", "HEAD"], cwd=ROOT,
+                                                     capture_output=True, text=True).stdout.strip() or "?"
     except Exception:
         rec["git_commit"] = "?"
     rec["command"] = command
-    # the timed launches are the last ones of each kernel (the shape sweep and
-    # the tuner come first): the median of the last three
-    rec["bytes_per_launch"][workload] = {
-        k: int(statistics.median([v[i] for i in sorted(v, key=int)[-3:]])) for k, v in per.items()}
+    # per template instance (launch shape), the median over its launches
+    rec["bytes_per_launch"][workload] = {k: int(statistics.median(v.values())) for k, v in per.items()}
     with open(TRAFFIC_RECORD, "w") as f:
         json.dump(rec, f, indent=1)
     return rec
@@ -439,7 +444,9 @@ def run_ours(args, rank, world, local_rank):
     # 16 B, occulter rows 32 B + 16 B, V 8 B / coefficients 8 B, image 4 B)
     alg_bytes = {"forward": J * 32 + K * 48 + G * 48 + K * 8,
                  "adjoint": J * 32 + K * 48 + G * 48 + K * 8 + J * 4}[dom]
-    traffic, traffic_src = measured_traffic(args.workload, f"k_{dom}")
+    masked = 1 if obs.refs is not None else 0
+    inst = (FWD_INSTANCES[shapes[0]] if dom == "forward" else ADJ_INSTANCES[shapes[1]]).format(m=masked)
+    traffic, traffic_src = measured_traffic(args.workload, inst)
     res = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -467,7 +474,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac_of_evaluated": round(dom_eval / dom_s / peak_terms, 4),
                      "algorithmic_bytes": alg_bytes,
                      "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
-                     "traffic_source": traffic_src},
+                     "traffic_source": traffic_src, "instance": inst},
         "kernel_ms": {"forward": round(fwd_s * 1e3, 3), "adjoint": round(adj_s * 1e3, 3)},
         "culling": {"forward_evaluated": round(ev_f / tot, 4), "forward_mixed": round(mx_f / tot, 4),
                     "adjoint_evaluated": round(ev_a / tot, 4), "adjoint_mixed": round(mx_a / tot, 4)},
@@ -611,7 +618,8 @@ def run_formation(args, rank, world, local_rank):
     total_s, e2e_s = replicas.max_over_ranks([total_s, e2e_s], device=dev)
     if rank != 0:
         return None
-    traffic, traffic_src = measured_traffic(args.workload, "k_form_forward" if fwd_s >= adj_s else "k_form_adjoint")
+    traffic, traffic_src = measured_traffic(
+        args.workload, f"k_form_{'forward' if fwd_s >= adj_s else 'adjoint'}<{plan.form_S}>")
     pk, pk_kind = peaks()
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_terms = 128 / FORM_FFMA_PER_TERM * nsm * pk["sm_max_mhz"] * 1e6
@@ -1057,6 +1065,7 @@ def main():
                     help="store the DRAM bytes per launch of an ncu --csv metrics log of this "
                          "workload as the traffic record of the current kernel sources, and exit")
     ap.add_argument("--record-command", default="", help="the ncu command line, stored with the record")
+    ap.add_argument("--record-commit", default="", help="the commit the capture ran on (default: HEAD)")
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOAD_TEXT),
                     help="benchmark configuration (default: the headline one)")
     ap.add_argument("--formation", action="store_true",
@@ -1067,7 +1076,8 @@ def main():
                     help="days of the stream workload")
     args = ap.parse_args()
     if args.record_traffic:
-        print(json.dumps(record_traffic(args.record_traffic, args.workload, args.record_command)))
+        print(json.dumps(record_traffic(args.record_traffic, args.workload, args.record_command,
+                                        args.record_commit)))
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -33,26 +33,28 @@ def _csv(tmp_path, rows):
 
 
 def test_traffic_record_roundtrip(bench, tmp_path):
-    fwd = "void viss::k_forward<256, 4, 2, true, false>(viss::FwdParams)"
-    adj = "void viss::k_adjoint<128, 8, 4, true, false>(viss::AdjParams)"
+    fwd = "void viss::k_forward<256, 4, 2, 1, 0>(viss::FwdParams)"   # as ncu names it
+    adj = "void viss::k_adjoint<128, 8, 4, 1, 0>(viss::AdjParams)"
     rows = []
-    for mb in (90, 100, 101, 102):             # four forward launches, the last three are timed
+    for mb in (90, 100, 101, 102):             # four launches of one forward instance
         rows += [(fwd, "dram__bytes_read.sum", "Mbyte", f"{mb}"), (fwd, "dram__bytes_write.sum", "byte", "1,000")]
     rows += [(adj, "dram__bytes_read.sum", "Gbyte", "0.5"), (adj, "dram__bytes_write.sum", "Mbyte", "2")]
-    form = "void viss::k_form_forward_split<10>(viss::FormParams)"
+    form = "void viss::k_form_forward<10>(viss::FormParams)"
     rows += [(form, "dram__bytes_read.sum", "Mbyte", "33"), (form, "dram__bytes_write.sum", "byte", "0")]
     rec = bench.record_traffic(_csv(tmp_path, rows), "c3_10mhz", "ncu ...")
-    assert rec["bytes_per_launch"]["c3_10mhz"]["k_forward"] == 101_001_000
-    assert rec["bytes_per_launch"]["c3_10mhz"]["k_adjoint"] == 502_000_000
-    assert rec["bytes_per_launch"]["c3_10mhz"]["k_form_forward"] == 33_000_000
-    v, src = bench.measured_traffic("c3_10mhz", "k_forward")
-    assert v == 101_001_000 and "these kernel sources" in src
-    assert bench.measured_traffic("c2", "k_forward")[0] is None
+    got = rec["bytes_per_launch"]["c3_10mhz"]
+    assert got["k_forward<256, 4, 2, 1, 0>"] == 100_501_000      # median of four launches
+    assert got["k_adjoint<128, 8, 4, 1, 0>"] == 502_000_000
+    assert got["k_form_forward<10>"] == 33_000_000
+    v, src = bench.measured_traffic("c3_10mhz", bench.FWD_INSTANCES[0].format(m=1))
+    assert v == 100_501_000 and "these kernel sources" in src
+    assert bench.measured_traffic("c3_10mhz", bench.FWD_INSTANCES[1].format(m=1))[0] is None
+    assert bench.measured_traffic("c2", "k_forward<256, 4, 2, 1, 0>")[0] is None
     # a record of other kernel sources is never reported
     d = json.loads(open(bench.TRAFFIC_RECORD).read())
     d["kernel_sources_sha256"] = "0" * 64
     open(bench.TRAFFIC_RECORD, "w").write(json.dumps(d))
-    v, src = bench.measured_traffic("c3_10mhz", "k_forward")
+    v, src = bench.measured_traffic("c3_10mhz", "k_forward<256, 4, 2, 1, 0>")
     assert v is None and "other kernel sources" in src
 
 

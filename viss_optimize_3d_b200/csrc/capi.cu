@@ -695,8 +695,7 @@ int viss_forward_formation(viss_plan *p, const float *sky, float *V, int flags, 
   const long long Tc = T / C;
   // about 16 waves of one block per SM, each block 8 snapshots of one channel
   // x a chunk of tiles
-  const int ns = viss::form_forward_snapshots_per_block(p->form_S);
-  const long long blocks = C * ((Tc + ns - 1) / ns);
+  const long long blocks = C * ((Tc + viss::kFormFwdNT / 32 - 1) / (viss::kFormFwdNT / 32));
   long long c = (16LL * p->nsm + blocks - 1) / blocks;
   c = std::max<long long>(1, std::min<long long>(c, std::max(1, p->ntiles / 4)));
   viss::FormParams fp = form_params(p, flags);

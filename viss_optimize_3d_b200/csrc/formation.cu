@@ -250,259 +250,6 @@ __global__ void __launch_bounds__(kFormFwdNT, 1) k_form_forward(const FormParams
   }
 }
 
-// ------------------------------------------------ forward, split snapshots
-// For S >= kFormSplitMinS the S(S-1)/2 pair accumulators no longer fit beside
-// enough warps (the one-warp-per-snapshot kernel above needs 240 registers at
-// S = 10, one CTA per SM).  Here two warps share a snapshot: warp half 0 owns
-// the pairs (a, b) with b <= bA, half 1 those with b > bA (bA chosen to split
-// the pairs evenly), so each keeps about half the accumulators.  Each half
-// evaluates half of the S exponentials of a 32-pixel group (half 0: b < S/2,
-// half 1: b >= S/2) and the two exchange them through shared memory; per group
-// the halves meet at an mbarrier of two arrivals (one per warp), double
-// buffered by the group's parity, every wait bounded like the stage ring's.
-// Both halves take the same tile and mode decisions (they classify the same
-// snapshot), so they pass the same sequence of groups.
-template <int S>
-__host__ __device__ constexpr int form_split_b() {
-  // the largest bA with bA(bA+1)/2 <= B/2, or the next one if that is closer
-  int b = 1;
-  while ((b + 1) * (b + 2) / 2 * 2 <= form_pairs(S)) ++b;
-  const int lo = b * (b + 1) / 2, hi = (b + 1) * (b + 2) / 2;
-  return (2 * hi - form_pairs(S) < form_pairs(S) - 2 * lo) ? b + 1 : b;
-}
-
-template <int S, int HALF>
-struct FormSplit {
-  static constexpr int bA = form_split_b<S>();
-  static constexpr int B0 = HALF == 0 ? 1 : bA + 1;          // first b of this half's pairs
-  static constexpr int B1 = HALF == 0 ? bA : S - 1;          // last b
-  static constexpr int NP = B1 * (B1 + 1) / 2 - (B0 - 1) * B0 / 2;  // pairs of this half
-  static constexpr int E0 = HALF == 0 ? 0 : S / 2;           // exponentials this half evaluates
-  static constexpr int E1 = HALF == 0 ? S / 2 : S;
-  // local index of pair (a, b), b in [B0, B1]
-  static __host__ __device__ constexpr int local(int a, int b) { return b * (b - 1) / 2 - (B0 - 1) * B0 / 2 + a; }
-};
-
-// One tile for the calling warp's half.  grp counts the 32-pixel groups this
-// pair of warps has exchanged so far.  Returns false if an exchange wait gave
-// up (the partner warp stopped).
-template <int S, int HALF, int MODE>
-__device__ __forceinline__ bool form_fwd_tile_split(const double4 *tp, const double4 *U,
-                                                    const double4 *rows, unsigned hid, unsigned mix,
-                                                    float2 (*xF)[S][32], uint64_t *xbar, int &grp,
-                                                    float (&ar)[FormSplit<S, HALF>::NP],
-                                                    float (&ai)[FormSplit<S, HALF>::NP]) {
-  using H = FormSplit<S, HALF>;
-  const int lane = threadIdx.x & 31;
-#pragma unroll 1
-  for (int q = 0; q < kTilePix / 32; ++q, ++grp) {
-    const int par = grp & 1;
-    const double4 rec = tp[q * 32 + lane];
-    const double x = rec.x, y = rec.y, z = rec.z;
-    float I = sky_bits(rec);
-    if (MODE == kMixed && ((mix >> S) & 1u)) I = visible_row(rows[S], x, y, z) ? I : 0.f;
-    float Fr[S], Fi[S];
-#pragma unroll
-    for (int b = H::E0; b < H::E1; ++b) {
-      float c, s;
-      sat_exp(U[b], x, y, z, c, s);
-      Fr[b] = c;
-      Fi[b] = -s;
-      if (MODE != kOpen) {
-        float m = ((hid >> b) & 1u) ? 0.f : 1.f;
-        if (MODE == kMixed && ((mix >> b) & 1u)) m = visible_row(rows[b], x, y, z) ? m : 0.f;
-        Fr[b] *= m;
-        Fi[b] *= m;
-      }
-      xF[par][b][lane] = make_float2(Fr[b], Fi[b]);
-    }
-    // both halves' exponentials of this group are in xF[par]
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&xbar[par]);
-    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&xbar[par], static_cast<uint32_t>(grp >> 1) & 1u)))
-      return false;
-#pragma unroll
-    for (int b = 0; b < S; ++b) {
-      if (b >= H::E0 && b < H::E1) continue;
-      if (b > H::B1) continue;
-      const float2 f = xF[par][b][lane];
-      Fr[b] = f.x;
-      Fi[b] = f.y;
-    }
-    float Gr[S - 1], Gi[S - 1];
-#pragma unroll
-    for (int a = 0; a < H::B1; ++a) {
-      Gr[a] = I * Fr[a];
-      Gi[a] = I * Fi[a];
-    }
-#pragma unroll
-    for (int b = H::B0; b <= H::B1; ++b) {
-      const float cr = Fr[b], ci = -Fi[b];   // conj(F_b)
-#pragma unroll
-      for (int a = 0; a < b; ++a) {
-        const int li = H::local(a, b);
-        ar[li] = fmaf(Gr[a], cr, fmaf(-Gi[a], ci, ar[li]));
-        ai[li] = fmaf(Gr[a], ci, fmaf(Gi[a], cr, ai[li]));
-      }
-    }
-  }
-  return true;
-}
-
-template <int S, int HALF>
-__device__ __forceinline__ void form_fwd_split_body(const FormParams &p, double4 (*s_pix)[kTilePix],
-                                                     const double4 *sU, const double4 *srow,
-                                                     const float4 *srow32, float2 (*xF)[S][32],
-                                                     uint64_t *xbar, uint64_t *s_full, uint64_t *s_empty,
-                                                     volatile int *abort_flag, bool tok, long long t,
-                                                     const double4 *pix, int t0, int ntile) {
-  using H = FormSplit<S, HALF>;
-  constexpr int ST = kFwdStages;
-  constexpr int NW = kFormFwdNT / 32;
-  constexpr uint32_t kTileBytes = kTilePix * sizeof(double4);
-  const int tid = threadIdx.x, lane = tid & 31;
-  auto issue = [&](int i, int stage) {
-    mbar_expect_tx(&s_full[stage], kTileBytes);
-    bulk_g2s(s_pix[stage], pix + static_cast<long long>(t0 + i) * kTilePix, kTileBytes, &s_full[stage]);
-  };
-  float ar[H::NP], ai[H::NP];
-#pragma unroll
-  for (int k = 0; k < H::NP; ++k) ar[k] = ai[k] = 0.f;
-  double sr = 0.0, si = 0.0;   // lane l keeps local pair l (NP <= 32)
-  auto fold = [&]() {
-#pragma unroll
-    for (int k = 0; k < H::NP; ++k) {
-      float vr = ar[k], vi = ai[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        vr += __shfl_xor_sync(0xffffffffu, vr, o);
-        vi += __shfl_xor_sync(0xffffffffu, vi, o);
-      }
-      if (lane == k) {
-        sr += vr;
-        si += vi;
-      }
-      ar[k] = ai[k] = 0.f;
-    }
-  };
-  unsigned long long evaluated = 0, mixed_terms = 0;
-  int next = 0, since_fold = 0, grp = 0;
-  for (int it = 0; it < ntile; ++it) {
-    const int tt = t0 + it, stage = it % ST;
-    if (tid == 0 && !ring_refill<ST>(s_empty, next, it, ntile, issue)) {
-      atomicOr(p.err, kErrTimeout);
-      *abort_flag = 1;
-    }
-    if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
-    unsigned hid, mix;
-    bool snap_hidden;
-    classify<S>(p.cones[tt], srow32, p.sat_rows, p.snap_rows, hid, mix, snap_hidden);
-    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_full[stage], static_cast<uint32_t>(it / ST) & 1u))) {
-      if (lane == 0) atomicOr(p.err, kErrTimeout);
-      *abort_flag = 1;
-      break;
-    }
-    if (tok && !snap_hidden && S - __popc(hid) >= 2) {
-      bool ok;
-      if (mix | hid) {
-        ok = form_fwd_tile_split<S, HALF, kMixed>(s_pix[stage], sU, srow, hid, mix, xF, xbar, grp, ar, ai);
-        mixed_terms += static_cast<unsigned long long>(kTilePix) * H::NP;
-      } else {
-        ok = form_fwd_tile_split<S, HALF, kOpen>(s_pix[stage], sU, srow, hid, mix, xF, xbar, grp, ar, ai);
-      }
-      if (!ok) {
-        if (lane == 0) atomicOr(p.err, kErrTimeout);
-        *abort_flag = 1;
-        break;
-      }
-      evaluated += static_cast<unsigned long long>(kTilePix) * H::NP;
-    }
-    ring_release(s_empty, stage);
-    if (++since_fold == kFormFoldTiles) {
-      fold();
-      since_fold = 0;
-    }
-  }
-  if (tid == 0) ring_drain<ST>(s_full, next);
-  fold();
-  if (p.counter && lane == 0) {
-    if (evaluated) atomicAdd(p.counter, evaluated);
-    if (mixed_terms) atomicAdd(p.counter + 2, mixed_terms);
-  }
-  if (!tok) return;
-  double2 *out = p.part_fwd + static_cast<long long>(blockIdx.y) * p.T * form_pairs(S) + t * form_pairs(S);
-#pragma unroll
-  for (int b = H::B0; b <= H::B1; ++b) {
-#pragma unroll
-    for (int a = 0; a < b; ++a)
-      if (lane == H::local(a, b)) out[pair_index<S>(a, b)] = make_double2(sr, si);
-  }
-  (void)NW;
-}
-
-template <int S>
-__global__ void __launch_bounds__(kFormFwdNT, 2) k_form_forward_split(const FormParams p) {
-  constexpr int NW = kFormFwdNT / 32;
-  constexpr int NS = NW / 2;   // snapshots per CTA (two warps each)
-  constexpr int ST = kFwdStages;
-  static_assert(FormSplit<S, 0>::NP <= 32 && FormSplit<S, 1>::NP <= 32, "a lane keeps one pair sum");
-  __shared__ __align__(128) double4 s_pix[ST][kTilePix];
-  __shared__ __align__(16) double4 s_U[NS][S];
-  __shared__ __align__(16) double4 s_row[NS][S + 1];
-  __shared__ __align__(16) float4 s_row32[NS][S + 1];
-  __shared__ __align__(16) float2 s_xF[NS][2][S][32];   // exchanged exponentials, by group parity
-  __shared__ __align__(8) uint64_t s_xbar[NS][2];
-  __shared__ __align__(8) uint64_t s_full[ST], s_empty[ST];
-  __shared__ int s_abort;
-  volatile int *abort_flag = &s_abort;
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int pr = warp >> 1, half = warp & 1;
-  const long long bpc = (p.Tc + NS - 1) / NS;
-  const long long ch = blockIdx.x / bpc;
-  const long long tl = (blockIdx.x - ch * bpc) * NS + pr;
-  const bool tok = tl < p.Tc;
-  const long long t = ch * p.Tc + tl;
-  const double4 pass = make_double4(0.0, 0.0, 0.0, -4.0);
-  if (half == 0) {
-    if (lane < S) s_U[pr][lane] = tok ? p.U[t * S + lane] : make_double4(0, 0, 0, 0);
-    if (lane <= S) {
-      double4 r = pass;
-      if (tok && lane < S && p.sat_rows) r = p.occ[t * S + lane];
-      if (tok && lane == S && p.snap_rows) r = p.occ[p.T * S + t];
-      s_row[pr][lane] = r;
-      float4 r32 = make_float4(0.f, 0.f, 0.f, -4.f);
-      if (tok && lane < S && p.sat_rows) r32 = p.occ32[t * S + lane];
-      if (tok && lane == S && p.snap_rows) r32 = p.occ32[p.T * S + t];
-      s_row32[pr][lane] = r32;
-    }
-  }
-  const int t0 = blockIdx.y * p.tiles_per_chunk;
-  const int ntile = max(0, min(t0 + p.tiles_per_chunk, p.ntiles) - t0);
-  if (tid == 0) {
-#pragma unroll
-    for (int s = 0; s < ST; ++s) {
-      mbar_init(&s_full[s], 1);
-      mbar_init(&s_empty[s], NW);
-    }
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      mbar_init(&s_xbar[k][0], 2);
-      mbar_init(&s_xbar[k][1], 2);
-    }
-    fence_mbar_init();
-    s_abort = 0;
-  }
-  __syncthreads();
-  const double4 *pix = p.pix + ch * p.Jpad;
-  if (half == 0)
-    form_fwd_split_body<S, 0>(p, s_pix, s_U[pr], s_row[pr], s_row32[pr], s_xF[pr], s_xbar[pr], s_full,
-                              s_empty, abort_flag, tok, t, pix, t0, ntile);
-  else
-    form_fwd_split_body<S, 1>(p, s_pix, s_U[pr], s_row[pr], s_row32[pr], s_xF[pr], s_xbar[pr], s_full,
-                              s_empty, abort_flag, tok, t, pix, t0, ntile);
-}
-
 // --------------------------------------------------------------- adjoint
 // A warp owns 32 * P pixels (P per lane); the CTA streams a chunk of
 // snapshots through a shared-memory ring, kFormSnapTile snapshots per stage
@@ -711,19 +458,11 @@ __global__ void __launch_bounds__(kFormAdjNT, 1) k_form_adjoint(const FormParams
 
 int form_adjoint_pixels_per_block() { return (kFormAdjNT / 32) * 32 * kFormAdjP; }
 
-int form_forward_snapshots_per_block(int S) {
-  return S >= kFormSplitMinS ? kFormFwdNT / 64 : kFormFwdNT / 32;
-}
-
 template <int S>
 static cudaError_t form_fwd_inst(const FormParams &p, int nchunk, cudaStream_t st) {
-  const int ns = form_forward_snapshots_per_block(S);
-  const long long gx = p.channels * ((p.Tc + ns - 1) / ns);
+  const long long gx = p.channels * ((p.Tc + kFormFwdNT / 32 - 1) / (kFormFwdNT / 32));
   if (gx > 0x7fffffffLL || nchunk > 65535) return cudaErrorInvalidValue;
-  if constexpr (S >= kFormSplitMinS)
-    k_form_forward_split<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormFwdNT, 0, st>>>(p);
-  else
-    k_form_forward<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormFwdNT, 0, st>>>(p);
+  k_form_forward<S><<<dim3(static_cast<unsigned>(gx), nchunk), kFormFwdNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -58,7 +58,6 @@ constexpr int kFormFwdNT = 256;    // forward: threads per block (one snapshot p
 constexpr int kFormAdjNT = 256;    // adjoint: threads per block
 constexpr int kFormSnapTile = 8;   // snapshots per adjoint staging tile
 constexpr int kFormFoldTiles = 32; // forward: pixel tiles between FP64 folds
-constexpr int kFormSplitMinS = 6;  // forward: from this S on, two warps share a snapshot
 __host__ __device__ constexpr int form_pairs(int S) { return S * (S - 1) / 2; }
 // Adjoint coefficient layout per snapshot: column b (pairs a < b, a = 0..b-1)
 // starts at form_col0(b) and is padded to an even length with zeros, so that
@@ -94,7 +93,6 @@ struct FormParams {
 cudaError_t launch_form_forward(const FormParams &p, int S, int nchunk, cudaStream_t st);
 cudaError_t launch_form_adjoint(const FormParams &p, int S, int nchunk, cudaStream_t st);
 int form_adjoint_pixels_per_block();
-int form_forward_snapshots_per_block(int S);
 
 struct FwdShape { int R, minb; };
 struct AdjShape { int P, minb; };
