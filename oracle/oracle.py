@@ -2,7 +2,7 @@
 viss_optimize_3d hot path.
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
-the CPU-baseline leg of bench.py, as the checker.  The product
+the CPU-baseline leg of bench.py, to check results and to time the CPU path.  The product
 (``viss_optimize_3d_b200``) never imports it.
 
 Each wrapper names the reference lines its C function restates (see the

@@ -1,7 +1,7 @@
 /*
  * viss_oracle.c -- CPU restatement of the viss_optimize_3d hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library:
+ * TEST INFRASTRUCTURE ONLY.  The CUDA library's results are tested against it:
  * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
  * it.  Nothing in the product (viss_optimize_3d_b200/, the C ABI, the host
  * executables) links or calls it.
