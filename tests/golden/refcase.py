@@ -28,8 +28,10 @@ def _fmt(x) -> str:
 
 
 def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10,
-              spacing=(40.0, 250.0), cross_sigma: float = 30.0):
-    """spacing: along-track gaps U(lo, hi) m; cross_sigma: cross-track jitter (m)."""
+              spacing=(40.0, 250.0), cross_sigma: float = 30.0, frequency: float = 1e7):
+    """spacing: along-track gaps U(lo, hi) m; cross_sigma: cross-track jitter (m);
+    frequency: the uvw rows are in wavelengths of the reference's FP32
+    lamda = 3e8 / frequency."""
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
     from oracle import oracle as O
@@ -65,7 +67,8 @@ def make_case(seed: int = 5, nside: int = 4, n_sat: int = 4, n_snap: int = 10,
             break
     else:
         raise RuntimeError("no geometry with a clear occultation margin")
-    u = ((rows_a - rows_b) / float(LAMBDA_10M)).astype(np.float32)
+    lam = np.float32(3e8 / np.float32(frequency))
+    u = ((rows_a - rows_b) / float(lam)).astype(np.float32)
     bll = np.linalg.norm(u.astype(np.float64), axis=1).astype(np.float32)
     uvw = np.concatenate([u, -u])
     xyza = np.concatenate([rows_a, rows_a]).astype(np.float32)
@@ -163,15 +166,26 @@ def write_inputs(case, root: str, variant_10m: bool = True, day: int = 1):
     return d
 
 
-def read_inputs(root: str, variant_10m: bool = True):
+def make_days_1m(days: int = 3):
+    """Three distinct days of the 1 MHz programs (vissgen3d_*, not _10m): the
+    same sky, a wider formation (0.4-2.5 km gaps, so |u| reaches ~20
+    wavelengths at 300 m) on a new seed each day; every (row, pixel) still
+    >= 1e-4 from the occultation cone."""
+    cases = [make_case(seed=20 + d, spacing=(400.0, 2500.0), cross_sigma=300.0, frequency=1e6)
+             for d in range(days)]
+    sky = {k: cases[0][k] for k in ("theta", "phi", "B")}
+    return [dict(c, **sky) for c in cases]
+
+
+def read_inputs(root: str, variant_10m: bool = True, day: int = 1):
     d = os.path.join(root, "earth_10Mhz" if variant_10m else "earth_1Mhz")
     suffix = "_10Mhz.txt" if variant_10m else ".txt"
     Bf = np.loadtxt(os.path.join(d, "B" + suffix), dtype=np.float32)
     case = dict(B=Bf[1:], theta=np.loadtxt(os.path.join(d, "theta_heal" + suffix), dtype=np.float32),
                 phi=np.loadtxt(os.path.join(d, "phi_heal" + suffix), dtype=np.float32))
     for name in ("uvw", "xyza", "xyzb"):
-        case[name] = np.loadtxt(os.path.join(d, name + "1day1M.txt"), dtype=np.float32)[1:]
-    case["bll"] = np.loadtxt(os.path.join(d, "bll1day1M.txt"), dtype=np.float32)[1:]
+        case[name] = np.loadtxt(os.path.join(d, f"{name}{day}day1M.txt"), dtype=np.float32)[1:]
+    case["bll"] = np.loadtxt(os.path.join(d, f"bll{day}day1M.txt"), dtype=np.float32)[1:]
     return case
 
 

@@ -97,3 +97,31 @@ def test_limb_bits_agree_outside_the_fp32_error_band(oracle):
     far = np.abs(margins) >= 5e-7
     assert far.sum() >= 4
     np.testing.assert_array_equal(ref_bits[far], our_bits[far])
+
+
+# ----------------------------------------------------- the 1 MHz program
+FIX1M = os.path.join(HERE, "golden", "ref_noblockage_1m")
+
+
+def test_1m_fixture_inputs_are_the_generator_days():
+    for d, gen in enumerate(refcase.make_days_1m(), start=1):
+        case = refcase.read_inputs(FIX1M, variant_10m=False, day=d)
+        for k in ("theta", "phi", "B", "uvw", "xyza", "xyzb", "bll"):
+            np.testing.assert_array_equal(case[k], gen[k])
+
+
+def test_oracle_reproduces_the_1m_reference_days(oracle):
+    """The reference's 1 MHz vissgen3d_noblockage (lamda = 300 m, 667 shells),
+    run over its 450 days: the oracle's restatement of vissGen reproduces its
+    images of days 1-3 and its printed forward visibilities of day 1."""
+    for d in (1, 2, 3):
+        case = refcase.read_inputs(FIX1M, variant_10m=False, day=d)
+        V0, C = refcase.oracle_vissgen(case, blockage=False, frequency=1e6)
+        Cref = np.loadtxt(os.path.join(FIX1M, "3dnoblockage", f"C{d}day1M.txt"))
+        assert Cref.shape == C.shape == (192,)
+        assert np.abs(C - Cref).max() <= 2e-5 * np.abs(Cref).max(), (d, np.abs(C - Cref).max())
+        if d == 1:
+            text = open(os.path.join(FIX1M, "reference_stdout_days1-3.txt")).read()
+            vals = re.findall(r"Viss\[(\d)\]: \(([^,]+),([^)]+)\)", text)[:3]
+            Vref = np.array([complex(float(a), float(b)) for _, a, b in vals])
+            np.testing.assert_allclose(V0[:3], Vref, rtol=2e-5, atol=2e-5 * np.abs(Vref).max())

@@ -159,3 +159,21 @@ def test_noblockage_10m_at_the_limb_differs_from_the_reference_only_by_its_fp32_
     assert np.abs(C - Co).max() <= 2e-5 * scale, np.abs(C - Co).max()
     flip = (our_bits.astype(float) - ref_bits.astype(float)) @ dC
     assert np.abs(C - (Cref + flip)).max() <= 4e-5 * scale, np.abs(C - (Cref + flip)).max()
+
+
+FIX1M = os.path.join(ROOT, "tests", "golden", "ref_noblockage_1m")
+
+
+def test_noblockage_1m_reproduces_reference_days(tmp_path, oracle):
+    """The 1 MHz drop-in (vissgen3d_noblockage) against the reference's own
+    1 MHz program on three days: its images C1..C3 to 2e-5 of the largest
+    value (the text's precision)."""
+    for d in (1, 2, 3):
+        refcase.write_inputs(refcase.read_inputs(FIX1M, variant_10m=False, day=d), str(tmp_path),
+                             variant_10m=False, day=d)
+    os.makedirs(tmp_path / "3dnoblockage")
+    run("vissgen3d_noblockage", tmp_path, "--days", "3")
+    for d in (1, 2, 3):
+        C = np.loadtxt(tmp_path / "3dnoblockage" / f"C{d}day1M.txt")
+        Cref = np.loadtxt(os.path.join(FIX1M, "3dnoblockage", f"C{d}day1M.txt"))
+        assert np.abs(C - Cref).max() <= 2e-5 * np.abs(Cref).max(), (d, np.abs(C - Cref).max())
