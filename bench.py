@@ -103,7 +103,8 @@ def measured_traffic(workload: str, kernel: str):
     v = rec.get("bytes_per_launch", {}).get(workload, {}).get(kernel)
     if v is None:
         return None, f"no ncu traffic record of {kernel} on {workload}"
-    return v, f"ncu capture of these kernel sources (git {rec.get('git_commit', '?')}): {rec.get('command', '')}"
+    cap = rec.get("captures", {}).get(workload, {})
+    return v, f"ncu capture of these kernel sources (git {cap.get('git_commit', '?')}): {cap.get('command', '')}"
 
 
 def record_traffic(csv_path: str, workload: str, command: str, commit: str = ""):
@@ -136,11 +137,11 @@ def record_traffic(csv_path: str, workload: str, command: str, commit: str = "")
     if rec.get("kernel_sources_sha256") != sha:
         rec = {"kernel_sources_sha256": sha, "bytes_per_launch": {}}
     try:
-        rec["git_commit"] = commit or subprocess.run(["git", "rev-parse", "--short", "HEAD"], cwd=ROOT,
-                                                     capture_output=True, text=True).stdout.strip() or "?"
+        git = commit or subprocess.run(["git", "rev-parse", "--short", "HEAD"], cwd=ROOT,
+                                       capture_output=True, text=True).stdout.strip() or "?"
     except Exception:
-        rec["git_commit"] = "?"
-    rec["command"] = command
+        git = "?"
+    rec.setdefault("captures", {})[workload] = {"git_commit": git, "command": command}
     # per template instance (launch shape), the median over its launches
     rec["bytes_per_launch"][workload] = {k: int(statistics.median(v.values())) for k, v in per.items()}
     with open(TRAFFIC_RECORD, "w") as f:

@@ -47,7 +47,7 @@ def test_traffic_record_roundtrip(bench, tmp_path):
     assert got["k_adjoint<128, 8, 4, 1, 0>"] == 502_000_000
     assert got["k_form_forward<10>"] == 33_000_000
     v, src = bench.measured_traffic("c3_10mhz", bench.FWD_INSTANCES[0].format(m=1))
-    assert v == 100_501_000 and "these kernel sources" in src
+    assert v == 100_501_000 and "these kernel sources" in src and "ncu ..." in src
     assert bench.measured_traffic("c3_10mhz", bench.FWD_INSTANCES[1].format(m=1))[0] is None
     assert bench.measured_traffic("c2", "k_forward<256, 4, 2, 1, 0>")[0] is None
     # a record of other kernel sources is never reported
