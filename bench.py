@@ -68,16 +68,22 @@ TRAFFIC_RECORD = os.path.join(ROOT, "viss_optimize_3d_b200", "ncu_traffic.json")
 BIG_WORKLOADS = ("prod_1mhz",)
 
 
+# the translation units of the kernels a traffic record measures (k_forward,
+# k_adjoint, k_form_forward, k_form_adjoint) and every header they include
+TRAFFIC_KERNEL_SOURCES = ("formation.cu", "visibility.cu", "visibility.cuh", "viss_common.cuh")
+
+
 def kernel_sources_sha() -> str:
-    """sha256 over the CUDA sources (csrc/*.cu, *.cuh) in name order: the key
-    under which a measured DRAM traffic record is valid."""
+    """sha256 over the CUDA sources of the recorded kernels (csrc/ files in
+    TRAFFIC_KERNEL_SOURCES, in name order): the key under which a measured
+    DRAM traffic record is valid.  Other sources (the gridded adjoint, the
+    HEALPix and staging kernels) do not enter these kernels' code."""
     import hashlib
     h = hashlib.sha256()
-    for name in sorted(os.listdir(KERNEL_SOURCES)):
-        if name.endswith((".cu", ".cuh")):
-            h.update(name.encode())
-            with open(os.path.join(KERNEL_SOURCES, name), "rb") as f:
-                h.update(f.read())
+    for name in sorted(TRAFFIC_KERNEL_SOURCES):
+        h.update(name.encode())
+        with open(os.path.join(KERNEL_SOURCES, name), "rb") as f:
+            h.update(f.read())
     return h.hexdigest()
 
 
@@ -918,6 +924,62 @@ def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
 
 
 # ---------------------------------------------------------- reference arm
+def run_gridded(args):
+    """The unmasked imaging adjoint (computeC of the noblockage programs) two
+    ways on one workload: the direct kernel (viss_adjoint, VISS_NO_MASK) and
+    per-facet type-3 NUFFTs (viss_adjoint_gridded, facet size chosen by the
+    library), CUDA events around each call, rel-L2 between the images."""
+    import torch
+    from viss_optimize_3d_b200 import pipeline, synth
+
+    dev = torch.device("cuda", 0)
+    name = args.workload
+    cfg = synth.CONFIGS[name]
+    obs = synth.make_observation(cfg)
+    g = pipeline.upload(obs, cfg.freqs_hz[0], device=dev)
+    K, J = g.plan.K, g.plan.J
+    gen = torch.Generator(device=dev).manual_seed(1)
+    a = torch.complex(torch.randn(K, device=dev, generator=gen), torch.randn(K, device=dev, generator=gen))
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ts = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return sorted(ts)[len(ts) // 2], out
+
+    steps = max(1, min(args.steps, 3))
+    for _ in range(max(1, min(args.warmup, 2))):
+        g.plan.adjoint(a, mask=False)
+        g.plan.adjoint_gridded(a)
+    t_direct, direct = timed(lambda: g.plan.adjoint(a, mask=False), steps)
+    t_grid, grid = timed(lambda: g.plan.adjoint_gridded(a), steps)
+    info = g.plan.gridded_info()
+    err = float(torch.linalg.norm((grid - direct).double()) / torch.linalg.norm(direct.double()))
+    terms = K * J
+    return {
+        "metric": "G uvw x pixel terms/s, unmasked imaging adjoint (computeC, noblockage), rel-L2<=1e-5",
+        "value": round(terms / t_grid / 1e9, 3), "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": max(1, min(args.warmup, 2)), "ms_per_step": round(t_grid * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64-phase/f32-grid", "data": "synthetic (seeded, see synth.py)",
+        "config": {"workload": WORKLOAD_TEXT.get(name, name), "pixels": J, "samples": K,
+                   "coefficients": "complex normal (seeded)"},
+        "direct": {"entry_point": "viss_adjoint (VISS_NO_MASK)", "ms": round(t_direct * 1e3, 2),
+                   "value": round(terms / t_direct / 1e9, 3)},
+        "gridded": {"entry_point": "viss_adjoint_gridded", "ms": round(t_grid * 1e3, 2),
+                    "facet_pixels": info["facet_pixels"], "facets": -(-J // info["facet_pixels"]),
+                    "grid": list(info["grid"]), "hbm_spread_blocks": info["hbm_blocks"]},
+        "speedup_gridded_vs_direct": round(t_direct / t_grid, 3),
+        "image_rel_l2_gridded_vs_direct": float(f"{err:.3e}"),
+    }
+
+
 def run_stream(args):
     """Observation days from files to images, wall clock, three ways on the same
     synthetic days: the text drop-in executable (the reference's interface and
@@ -1075,6 +1137,8 @@ def main():
                     help="skip timing the formation entry points beside the headline step")
     ap.add_argument("--stream-days", type=int, default=4,
                     help="days of the stream workload")
+    ap.add_argument("--gridded", action="store_true",
+                    help="time the unmasked imaging adjoint direct vs gridded (per-facet NUFFT) on --workload")
     args = ap.parse_args()
     if args.record_traffic:
         print(json.dumps(record_traffic(args.record_traffic, args.workload, args.record_command,
@@ -1106,6 +1170,10 @@ def main():
             return
         if args.workload == "stream":
             print(json.dumps(run_stream(args)), flush=True)
+            return
+        if args.gridded:
+            if rank == 0:
+                print(json.dumps(run_gridded(args)), flush=True)
             return
         res = run_ours(args, rank, world, local_rank)
         if not args.formation and args.formation_compare and args.workload in ("c1", "c2", "c3_10mhz", "c3_1mhz", "c3_small"):  # noqa: E501

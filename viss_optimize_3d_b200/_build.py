@@ -24,7 +24,7 @@ LIB = os.path.join(PKG, "libviss.so")
 BIN = os.path.join(PKG, "bin")
 
 CU_SOURCES = ["healpix.cu", "geometry.cu", "visibility.cu", "dcf.cu", "capi.cu", "noalloc.cu",
-              "days.cu", "formation.cu"]
+              "days.cu", "formation.cu", "gridded.cu"]
 HEADERS = ["viss_common.cuh", "visibility.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,7 +73,7 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_verbose: boo
             for out in ex.map(lambda c: _run(c, verbose), jobs):
                 logs.append(out)
     if force or jobs or _newer(LIB, objs):
-        _run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl",
+        _run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lcufft", "-lrt", "-ldl",
                                                                  "-lpthread"], verbose)
     if ptxas_verbose:
         print("\n".join(logs))

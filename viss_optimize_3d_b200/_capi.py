@@ -59,6 +59,8 @@ _SIGS = {
     "viss_plan_set_samples": (_i, [_v, _i64, _v, _v, _v, _i64, _v, _v]),
     "viss_forward": (_i, [_v, _v, _v, _i, _v]),
     "viss_adjoint": (_i, [_v, _v, _v, _f, _i, _v]),
+    "viss_adjoint_gridded": (_i, [_v, _v, _v, _f, _i, _i64, _v]),
+    "viss_plan_gridded_info": (_i, [_v, _v, _v, _v]),
     "viss_plan_last_counts": (_i, [_v, C.POINTER(_i64), C.POINTER(_i64)]),
     "viss_plan_tune": (_i, [_v, _v, _v, _v, _v, _i, C.POINTER(_i), C.POINTER(_i), _v]),
     "viss_plan_set_shapes": (_i, [_v, _i, _i]),

@@ -228,6 +228,36 @@ class Plan:
                                self._flags(fp64, mask, use_offset), _stream(coef)), "viss_adjoint")
         return out
 
+    def adjoint_gridded(self, coef, scale: float = 1.0, use_offset: bool = True, facet_pixels: int = 0,
+                        out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
+        """The unmasked adjoint (computeC of the noblockage programs,
+        vissgen3d_noblockage.cu:167-182) through per-facet type-3 NUFFTs
+        (viss_adjoint_gridded): the image of adjoint(coef, scale, mask=False)
+        to ~1e-6 relative.  facet_pixels = 0 lets the library choose; with
+        accumulate the image is added to `out`.  Synchronous."""
+        coef = _cuda(coef, torch.complex64, self.device)
+        if coef.shape != (self.K,):
+            raise ValueError(f"coef must have shape ({self.K},)")
+        if self.channels != 1:
+            raise ValueError("the gridded adjoint takes one channel")
+        if out is None:
+            out = torch.empty(self.J, dtype=torch.float32, device=self.device)
+        elif (out.dtype != torch.float32 or not out.is_contiguous() or out.numel() != self.J
+              or out.device != self.device):
+            raise ValueError(f"out must be a contiguous float32 tensor of {self.J} values on {self.device}")
+        flags = self._flags(False, False, use_offset, accumulate)
+        check(lib.viss_adjoint_gridded(self._h, _p(coef), _p(out), float(scale), flags, int(facet_pixels),
+                                       _stream(coef)), "viss_adjoint_gridded")
+        return out
+
+    def gridded_info(self) -> dict:
+        """What the last adjoint_gridded used: facet size, grid dimensions and
+        the spreading blocks that did not fit one shared-memory box."""
+        fp, hbm = C.c_int64(), C.c_int64()
+        dims = (C.c_int32 * 3)()
+        check(lib.viss_plan_gridded_info(self._h, C.byref(fp), dims, C.byref(hbm)), "viss_plan_gridded_info")
+        return {"facet_pixels": fp.value, "grid": tuple(dims), "hbm_blocks": hbm.value}
+
     # ---------------------------------------------------- formation mode
     def set_formation(self, U, off=None, occ_sat=None, occ_snap=None):
         """Samples of a satellite formation (viss_plan_set_formation): U is

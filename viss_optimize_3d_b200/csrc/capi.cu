@@ -53,6 +53,11 @@ cudaError_t launch_weights(long long, const float *, const float *, const int32_
 cudaError_t launch_wrot(long long, const float *, float2 *, cudaStream_t);
 cudaError_t launch_conj_mirror(long long, float2 *, cudaStream_t);
 cudaError_t launch_scale_coef(long long, const float *, const float2 *, float2 *, cudaStream_t);
+int gridded_adjoint(void **state, long long J, const double4 *pix, const int *perm, long long K,
+                    const double4 *samp, const float2 *coef, int use_off, long long facet_pix, float scale,
+                    float *img, int accumulate, long long max_cells, cudaStream_t st, int *grid_dims,
+                    long long *facet_used, long long *info);
+void gridded_free(void *state);
 }  // namespace viss
 
 #include "visibility.cuh"
@@ -168,6 +173,11 @@ struct viss_plan {
   int drop_tile = -1;  // test hook for the next kernel (viss_plan_debug_drop_copy)
   int fwd_waves = 16;
   int adj_waves = 16;
+  // viss_adjoint_gridded: its buffers and FFT plan, and what the last call used
+  void *gridded = nullptr;
+  int gridded_dims[3] = {0, 0, 0};
+  long long gridded_facet = 0;
+  long long gridded_hbm_blocks = 0;
 };
 
 namespace {
@@ -342,6 +352,7 @@ int viss_plan_destroy(viss_plan *p) {
                   p->form_coef};
   for (void *b : bufs)
     if (b) cudaFree(b);
+  if (p->gridded) viss::gridded_free(p->gridded);
   delete p;
   return VISS_OK;
 }
@@ -759,6 +770,42 @@ int viss_adjoint_formation(viss_plan *p, const float *coef, float *image, float 
             "viss_adjoint_formation: reduce");
   p->last_total = T * B * p->J;
   p->last_stream = st;
+  return VISS_OK;
+}
+
+// ------------------------------------------------------ gridded adjoint
+int viss_adjoint_gridded(viss_plan *p, const float *coef, float *image, float scale, int flags,
+                         int64_t facet_pixels, void *stream) {
+  const NvtxRange range("viss_adjoint_gridded");
+  if (!p || !coef || !image) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: bad arguments");
+  if (p->J <= 0 || p->K <= 0) return fail(VISS_ERR_STATE, "viss_adjoint_gridded: pixels or samples not set");
+  if (flags & VISS_FP64) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: split precision only");
+  if (p->has_refs && !(flags & VISS_NO_MASK))
+    return fail(VISS_ERR_ARG, "viss_adjoint_gridded: the gridded adjoint is unmasked; pass VISS_NO_MASK "
+                              "(or use viss_adjoint for occulted imaging)");
+  if (p->channels != 1) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: one channel only");
+  if (facet_pixels < 0) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: facet_pixels must be >= 0");
+  const long long max_cells = 1LL << 29;   // 4 GiB of FP32 complex grid
+  long long fp = facet_pixels, info = 0;
+  const cudaStream_t st = as_stream(stream);
+  VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
+            "viss_adjoint_gridded: coef");
+  const int s = viss::gridded_adjoint(&p->gridded, p->J, p->pix, p->perm, p->K, p->samp, p->coef,
+                                      (flags & VISS_NO_OFFSET) ? 0 : 1, fp, scale, image,
+                                      (flags & VISS_ACCUMULATE) ? 1 : 0, max_cells, st, p->gridded_dims, &fp,
+                                      &info);
+  p->gridded_facet = fp;
+  p->gridded_hbm_blocks = info;
+  p->last_stream = st;
+  return s;
+}
+
+int viss_plan_gridded_info(viss_plan *p, int64_t *facet_pixels, int32_t *grid_dims, int64_t *hbm_blocks) {
+  if (!p) return fail(VISS_ERR_ARG, "viss_plan_gridded_info: null plan");
+  if (facet_pixels) *facet_pixels = p->gridded_facet;
+  if (grid_dims)
+    for (int d = 0; d < 3; ++d) grid_dims[d] = p->gridded_dims[d];
+  if (hbm_blocks) *hbm_blocks = p->gridded_hbm_blocks;
   return VISS_OK;
 }
 
