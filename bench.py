@@ -89,13 +89,13 @@ def kernel_sources_sha() -> str:
 
 FWD_INSTANCES = ["k_forward<256, 4, 2, {m}, 0>", "k_forward<256, 4, 3, {m}, 0>",
                  "k_forward<256, 2, 3, {m}, 0>", "k_forward<256, 2, 4, {m}, 0>"]
-ADJ_INSTANCES = ["k_adjoint<128, 8, 4, {m}, 0>", "k_adjoint<128, 8, 5, {m}, 0>",
-                 "k_adjoint<128, 4, 5, {m}, 0>", "k_adjoint<128, 4, 6, {m}, 0>"]
+ADJ_INSTANCES = ["k_adjoint<128, 8, 4, {m}, 0, 0>", "k_adjoint<128, 8, 5, {m}, 0, 0>",
+                 "k_adjoint<128, 4, 5, {m}, 0, 0>", "k_adjoint<128, 4, 6, {m}, 0, 0>"]
 
 
 def measured_traffic(workload: str, kernel: str):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
-    of the kernel instance `kernel` (e.g. "k_adjoint<128, 8, 4, 1, 0>", the
+    of the kernel instance `kernel` (e.g. "k_adjoint<128, 8, 4, 1, 0, 0>", the
     launch shape the run used) on `workload`, from an ncu capture recorded by
     `bench.py --record-traffic`, or None when no capture of the current
     kernel sources exists (a record of other sources is never reported)."""
@@ -131,7 +131,7 @@ def record_traffic(csv_path: str, workload: str, command: str, commit: str = "")
         scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
         m = re.search(r"\b((?:k_form_forward|k_form_adjoint|k_forward|k_adjoint)<[^>]*>)", name)
         if m:
-            k = m.group(1)     # the template instance, e.g. k_adjoint<128, 8, 4, 1, 0>
+            k = m.group(1)     # the template instance, e.g. k_adjoint<128, 8, 4, 1, 0, 0>
             per.setdefault(k, {}).setdefault(row.get("ID"), 0.0)
             per[k][row.get("ID")] += float(val) * scale
     try:
@@ -925,10 +925,12 @@ def cpu_baseline(obs, f_hz, budget_s: float = 15.0):
 
 # ---------------------------------------------------------- reference arm
 def run_gridded(args):
-    """The unmasked imaging adjoint (computeC of the noblockage programs) two
-    ways on one workload: the direct kernel (viss_adjoint, VISS_NO_MASK) and
-    per-facet type-3 NUFFTs (viss_adjoint_gridded, facet size chosen by the
-    library), CUDA events around each call, rel-L2 between the images."""
+    """The imaging adjoint two ways on one workload, unmasked (computeC of the
+    noblockage programs) and occulted (of the blockage programs): the direct
+    kernel (viss_adjoint) and per-facet type-3 NUFFTs (viss_adjoint_gridded,
+    facet size chosen by the library; occulted: the pairs whose facet the
+    sample sees wholly gridded, the rest direct).  CUDA events around each
+    call, rel-L2 between the images."""
     import torch
     from viss_optimize_3d_b200 import pipeline, synth
 
@@ -941,8 +943,12 @@ def run_gridded(args):
     gen = torch.Generator(device=dev).manual_seed(1)
     a = torch.complex(torch.randn(K, device=dev, generator=gen), torch.randn(K, device=dev, generator=gen))
     stream = torch.cuda.current_stream(dev)
+    steps = max(1, min(args.steps, 3))
+    warm = max(1, min(args.warmup, 2))
 
-    def timed(fn, steps):
+    def timed(fn):
+        for _ in range(warm):
+            fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ts = []
         for _ in range(steps):
@@ -954,30 +960,30 @@ def run_gridded(args):
             ts.append(e0.elapsed_time(e1) / 1e3)
         return sorted(ts)[len(ts) // 2], out
 
-    steps = max(1, min(args.steps, 3))
-    for _ in range(max(1, min(args.warmup, 2))):
-        g.plan.adjoint(a, mask=False)
-        g.plan.adjoint_gridded(a)
-    t_direct, direct = timed(lambda: g.plan.adjoint(a, mask=False), steps)
-    t_grid, grid = timed(lambda: g.plan.adjoint_gridded(a), steps)
-    info = g.plan.gridded_info()
-    err = float(torch.linalg.norm((grid - direct).double()) / torch.linalg.norm(direct.double()))
     terms = K * J
-    return {
-        "metric": "G uvw x pixel terms/s, unmasked imaging adjoint (computeC, noblockage), rel-L2<=1e-5",
-        "value": round(terms / t_grid / 1e9, 3), "unit": UNIT, "n_gpus": 1, "steps": steps,
-        "warmup": max(1, min(args.warmup, 2)), "ms_per_step": round(t_grid * 1e3, 2), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64-phase/f32-grid", "data": "synthetic (seeded, see synth.py)",
-        "config": {"workload": WORKLOAD_TEXT.get(name, name), "pixels": J, "samples": K,
-                   "coefficients": "complex normal (seeded)"},
-        "direct": {"entry_point": "viss_adjoint (VISS_NO_MASK)", "ms": round(t_direct * 1e3, 2),
-                   "value": round(terms / t_direct / 1e9, 3)},
-        "gridded": {"entry_point": "viss_adjoint_gridded", "ms": round(t_grid * 1e3, 2),
-                    "facet_pixels": info["facet_pixels"], "facets": -(-J // info["facet_pixels"]),
-                    "grid": list(info["grid"]), "hbm_spread_blocks": info["hbm_blocks"]},
-        "speedup_gridded_vs_direct": round(t_direct / t_grid, 3),
-        "image_rel_l2_gridded_vs_direct": float(f"{err:.3e}"),
-    }
+    res = {"metric": "G uvw x pixel terms/s, occulted imaging adjoint (computeC), rel-L2<=1e-5", "unit": UNIT,
+           "n_gpus": 1, "steps": steps, "warmup": warm, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64-phase/f32-grid", "data": "synthetic (seeded, see synth.py)",
+           "config": {"workload": WORKLOAD_TEXT.get(name, name), "pixels": J, "samples": K,
+                      "coefficients": "complex normal (seeded)"}}
+    for label, mask in (("unmasked", False), ("occulted", True)):
+        t_direct, direct = timed(lambda: g.plan.adjoint(a, mask=mask))
+        t_grid, grid = timed(lambda: g.plan.adjoint_gridded(a, mask=mask))
+        info = g.plan.gridded_info()
+        err = float(torch.linalg.norm((grid - direct).double()) / torch.linalg.norm(direct.double()))
+        res[label] = {
+            "direct": {"entry_point": "viss_adjoint" + ("" if mask else " (VISS_NO_MASK)"),
+                       "ms": round(t_direct * 1e3, 2), "value": round(terms / t_direct / 1e9, 3)},
+            "gridded": {"entry_point": "viss_adjoint_gridded" + ("" if mask else " (VISS_NO_MASK)"),
+                        "ms": round(t_grid * 1e3, 2), "value": round(terms / t_grid / 1e9, 3),
+                        "facet_pixels": info["facet_pixels"], "facets": -(-J // info["facet_pixels"]),
+                        "grid": list(info["grid"]), "hbm_spread_blocks": info["hbm_blocks"]},
+            "speedup_gridded_vs_direct": round(t_direct / t_grid, 3),
+            "image_rel_l2_gridded_vs_direct": float(f"{err:.3e}"),
+        }
+    res["value"] = res["occulted"]["gridded"]["value"]
+    res["ms_per_step"] = res["occulted"]["gridded"]["ms"]
+    return res
 
 
 def run_stream(args):
@@ -1138,7 +1144,8 @@ def main():
     ap.add_argument("--stream-days", type=int, default=4,
                     help="days of the stream workload")
     ap.add_argument("--gridded", action="store_true",
-                    help="time the unmasked imaging adjoint direct vs gridded (per-facet NUFFT) on --workload")
+                    help="time the imaging adjoint (unmasked and occulted) direct vs gridded (per-facet NUFFT) "
+                         "on --workload")
     args = ap.parse_args()
     if args.record_traffic:
         print(json.dumps(record_traffic(args.record_traffic, args.workload, args.record_command,

@@ -34,7 +34,7 @@ def _csv(tmp_path, rows):
 
 def test_traffic_record_roundtrip(bench, tmp_path):
     fwd = "void viss::k_forward<256, 4, 2, 1, 0>(viss::FwdParams)"   # as ncu names it
-    adj = "void viss::k_adjoint<128, 8, 4, 1, 0>(viss::AdjParams)"
+    adj = "void viss::k_adjoint<128, 8, 4, 1, 0, 0>(viss::AdjParams)"
     rows = []
     for mb in (90, 100, 101, 102):             # four launches of one forward instance
         rows += [(fwd, "dram__bytes_read.sum", "Mbyte", f"{mb}"), (fwd, "dram__bytes_write.sum", "byte", "1,000")]
@@ -44,7 +44,7 @@ def test_traffic_record_roundtrip(bench, tmp_path):
     rec = bench.record_traffic(_csv(tmp_path, rows), "c3_10mhz", "ncu ...")
     got = rec["bytes_per_launch"]["c3_10mhz"]
     assert got["k_forward<256, 4, 2, 1, 0>"] == 100_501_000      # median of four launches
-    assert got["k_adjoint<128, 8, 4, 1, 0>"] == 502_000_000
+    assert got["k_adjoint<128, 8, 4, 1, 0, 0>"] == 502_000_000
     assert got["k_form_forward<10>"] == 33_000_000
     v, src = bench.measured_traffic("c3_10mhz", bench.FWD_INSTANCES[0].format(m=1))
     assert v == 100_501_000 and "these kernel sources" in src and "ncu ..." in src

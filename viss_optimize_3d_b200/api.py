@@ -228,13 +228,18 @@ class Plan:
                                self._flags(fp64, mask, use_offset), _stream(coef)), "viss_adjoint")
         return out
 
-    def adjoint_gridded(self, coef, scale: float = 1.0, use_offset: bool = True, facet_pixels: int = 0,
-                        out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
-        """The unmasked adjoint (computeC of the noblockage programs,
-        vissgen3d_noblockage.cu:167-182) through per-facet type-3 NUFFTs
-        (viss_adjoint_gridded): the image of adjoint(coef, scale, mask=False)
-        to ~1e-6 relative.  facet_pixels = 0 lets the library choose; with
-        accumulate the image is added to `out`.  Synchronous."""
+    def adjoint_gridded(self, coef, scale: float = 1.0, mask: bool = True, use_offset: bool = True,
+                        facet_pixels: int = 0, out: torch.Tensor | None = None,
+                        accumulate: bool = False) -> torch.Tensor:
+        """The imaging adjoint through per-facet type-3 NUFFTs
+        (viss_adjoint_gridded): the image of adjoint(coef, scale, mask=mask)
+        to ~1e-6 relative.  Unmasked (or a plan without occulter refs): computeC
+        of the noblockage programs (vissgen3d_noblockage.cu:167-182), all
+        gridded.  Occulted: computeC of the blockage programs
+        (vissgen3d_blockage.cu:167-192), the pairs whose facet the sample sees
+        wholly gridded and the rest through the direct kernel.  facet_pixels
+        = 0 lets the library choose (occulted: a multiple of 256); with
+        accumulate the image is added to `out`."""
         coef = _cuda(coef, torch.complex64, self.device)
         if coef.shape != (self.K,):
             raise ValueError(f"coef must have shape ({self.K},)")
@@ -245,7 +250,7 @@ class Plan:
         elif (out.dtype != torch.float32 or not out.is_contiguous() or out.numel() != self.J
               or out.device != self.device):
             raise ValueError(f"out must be a contiguous float32 tensor of {self.J} values on {self.device}")
-        flags = self._flags(False, False, use_offset, accumulate)
+        flags = self._flags(False, mask, use_offset, accumulate)
         check(lib.viss_adjoint_gridded(self._h, _p(coef), _p(out), float(scale), flags, int(facet_pixels),
                                        _stream(coef)), "viss_adjoint_gridded")
         return out

@@ -56,7 +56,8 @@ cudaError_t launch_scale_coef(long long, const float *, const float2 *, float2 *
 int gridded_adjoint(void **state, long long J, const double4 *pix, const int *perm, long long K,
                     const double4 *samp, const float2 *coef, int use_off, long long facet_pix, float scale,
                     float *img, int accumulate, long long max_cells, cudaStream_t st, int *grid_dims,
-                    long long *facet_used, long long *info);
+                    long long *facet_used, long long *info, const int4 *refs, const float4 *occ32,
+                    const float4 **fcones_out);
 void gridded_free(void *state);
 }  // namespace viss
 
@@ -502,8 +503,12 @@ int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stre
   return forward_impl(p, sky, V, flags, as_stream(stream), p->fwd_shape);
 }
 
+// fcones non-null: the hybrid instance (occulted, split precision), which
+// leaves the (sample, facet) pairs of wholly visible facets to the gridded
+// adjoint; facets of facet_pix records, nfacets of them.
 static int adjoint_impl(viss_plan *p, const float *coef, float *image, float scale, int flags,
-                        cudaStream_t st, int shape) {
+                        cudaStream_t st, int shape, const float4 *fcones = nullptr, long long facet_pix = 0,
+                        long long nfacets = 0) {
   const bool fp64 = (flags & VISS_FP64) != 0;
   const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
   int spc = 0;
@@ -533,7 +538,15 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
   ap.nchunk = nchunk;
   ap.drop_tile = p->drop_tile;
   p->drop_tile = -1;
-  VISS_CUDA(viss::launch_adjoint(ap, shape, nchunk, masked, fp64, st), "viss_adjoint: kernel");
+  if (fcones) {
+    if (!masked || fp64) return fail(VISS_ERR_ARG, "viss_adjoint: the hybrid adjoint is occulted split precision");
+    ap.fcones = fcones;
+    ap.facet_pix = facet_pix;
+    ap.nfacets = nfacets;
+    VISS_CUDA(viss::launch_adjoint_hybrid(ap, shape, nchunk, st), "viss_adjoint_gridded: direct kernel");
+  } else {
+    VISS_CUDA(viss::launch_adjoint(ap, shape, nchunk, masked, fp64, st), "viss_adjoint: kernel");
+  }
   VISS_CUDA(viss::launch_reduce_adj(p->J, p->Jpad, nchunk, p->channels, ap.part, p->perm, scale, image,
                                     (flags & VISS_ACCUMULATE) ? 1 : 0, st),
             "viss_adjoint: reduce");
@@ -780,24 +793,29 @@ int viss_adjoint_gridded(viss_plan *p, const float *coef, float *image, float sc
   if (!p || !coef || !image) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: bad arguments");
   if (p->J <= 0 || p->K <= 0) return fail(VISS_ERR_STATE, "viss_adjoint_gridded: pixels or samples not set");
   if (flags & VISS_FP64) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: split precision only");
-  if (p->has_refs && !(flags & VISS_NO_MASK))
-    return fail(VISS_ERR_ARG, "viss_adjoint_gridded: the gridded adjoint is unmasked; pass VISS_NO_MASK "
-                              "(or use viss_adjoint for occulted imaging)");
   if (p->channels != 1) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: one channel only");
   if (facet_pixels < 0) return fail(VISS_ERR_ARG, "viss_adjoint_gridded: facet_pixels must be >= 0");
+  const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
+  if (masked && !(p->max_turns < viss::kMaxTurns))
+    return fail(VISS_ERR_ARG, "viss_adjoint_gridded: |u|+|v|+|w|+|off| exceeds 2^28 turns");
   const long long max_cells = 1LL << 29;   // 4 GiB of FP32 complex grid
   long long fp = facet_pixels, info = 0;
   const cudaStream_t st = as_stream(stream);
   VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
             "viss_adjoint_gridded: coef");
+  const float4 *fcones = nullptr;
   const int s = viss::gridded_adjoint(&p->gridded, p->J, p->pix, p->perm, p->K, p->samp, p->coef,
                                       (flags & VISS_NO_OFFSET) ? 0 : 1, fp, scale, image,
                                       (flags & VISS_ACCUMULATE) ? 1 : 0, max_cells, st, p->gridded_dims, &fp,
-                                      &info);
+                                      &info, masked ? p->refs : nullptr, masked ? p->occ32 : nullptr, &fcones);
   p->gridded_facet = fp;
   p->gridded_hbm_blocks = info;
   p->last_stream = st;
-  return s;
+  if (s != VISS_OK || !masked) return s;
+  // the occulted adjoint: the direct kernel adds every pair the gridded part
+  // left out (facets the sample does not see wholly)
+  return adjoint_impl(p, coef, image, scale, (flags & ~VISS_FP64) | VISS_ACCUMULATE, st, p->adj_shape, fcones, fp,
+                      (p->J + fp - 1) / fp);
 }
 
 int viss_plan_gridded_info(viss_plan *p, int64_t *facet_pixels, int32_t *grid_dims, int64_t *hbm_blocks) {

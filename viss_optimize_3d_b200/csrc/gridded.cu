@@ -67,6 +67,7 @@ constexpr int kSpreadWarps = 8;
 constexpr int kSpreadP = 32 * kSpreadWarps;   // samples per spreading block
 constexpr int kBoxCells = 8192;               // shared-memory box capacity (complex points)
 constexpr int kW3 = 3 * kGridW;               // kernel weights per sample
+constexpr int kHybridAlign = 256;             // occulted plans: facets are whole direct-adjoint warp tiles
 constexpr size_t kSpreadSmem = 2 * sizeof(float) * kBoxCells + sizeof(float) * kSpreadP * kW3 +
                                sizeof(int) * kSpreadP * 4 + sizeof(float2) * kSpreadP;
 
@@ -121,8 +122,13 @@ __device__ double block_max(double v, double *red) {
 // pixel records.  Centre = normalised mean direction; e1, e2 complete a
 // right-handed frame; then the extents of the local coordinates, also folded
 // into xmax[0..2] (the bits of non-negative doubles order like the values).
+//
+// It also writes the facet's FP32 bounding cone (centre rounded to FP32, and
+// the largest chord from it to a pixel plus the classification margin,
+// rounded up; 4 for a facet whose mean direction is ~0, NaN if a pixel is
+// NaN): the cone the occulted (hybrid) path classifies samples against.
 __global__ void k_facet_frames(long long J, long long fp, const double4 *pix, FacetFrame *out,
-                               unsigned long long *xmax) {
+                               unsigned long long *xmax, float4 *fcones) {
   __shared__ double red[32];
   const long long f = blockIdx.x;
   const long long r0 = f * fp, r1 = min(J, r0 + fp);
@@ -139,6 +145,10 @@ __global__ void k_facet_frames(long long J, long long fp, const double4 *pix, Fa
   double nrm = sqrt(sx * sx + sy * sy + sz * sz);
   double c[3] = {0.0, 0.0, 1.0};
   if (nrm > 0) c[0] = sx / nrm, c[1] = sy / nrm, c[2] = sz / nrm;
+  const bool degenerate = !(nrm > 1e-6);
+  const float4 cf = degenerate ? make_float4(1.f, 0.f, 0.f, 0.f)
+                               : make_float4(__double2float_rn(c[0]), __double2float_rn(c[1]),
+                                             __double2float_rn(c[2]), 0.f);
   // e1 = normalise(c x a) with a the axis least aligned with c
   double a[3] = {1.0, 0.0, 0.0};
   if (fabs(c[0]) > 0.9) a[0] = 0.0, a[1] = 1.0;
@@ -146,9 +156,12 @@ __global__ void k_facet_frames(long long J, long long fp, const double4 *pix, Fa
   nrm = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
   for (int d = 0; d < 3; ++d) e1[d] /= nrm;
   const double e2[3] = {c[1] * e1[2] - c[2] * e1[1], c[2] * e1[0] - c[0] * e1[2], c[0] * e1[1] - c[1] * e1[0]};
-  double mx = 0, my = 0, zlo = 1e300, zhi = -1e300;
+  double mx = 0, my = 0, zlo = 1e300, zhi = -1e300, rho = 0, nan_px = 0;
   for (long long i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
     const double4 p = pix[i];
+    const double dx = p.x - cf.x, dy = p.y - cf.y, dz = p.z - cf.z;
+    rho = fmax(rho, sqrt(dx * dx + dy * dy + dz * dz));
+    if (isnan(p.x) || isnan(p.y) || isnan(p.z)) nan_px = 1;
     mx = fmax(mx, fabs(p.x * e1[0] + p.y * e1[1] + p.z * e1[2]));
     my = fmax(my, fabs(p.x * e2[0] + p.y * e2[1] + p.z * e2[2]));
     const double z = p.x * c[0] + p.y * c[1] + p.z * c[2] - 1.0;
@@ -159,7 +172,12 @@ __global__ void k_facet_frames(long long J, long long fp, const double4 *pix, Fa
   my = block_max(my, red);
   zhi = block_max(zhi, red);
   zlo = -block_max(-zlo, red);
+  rho = block_max(rho, red);
+  nan_px = block_max(nan_px, red);
   if (threadIdx.x == 0) {
+    float4 cone = cf;
+    cone.w = nan_px > 0 ? __int_as_float(0x7fc00000) : (degenerate ? 4.f : __double2float_ru(rho + kConeMargin32));
+    fcones[f] = cone;
     FacetFrame fr;
     for (int d = 0; d < 3; ++d) fr.e1[d] = e1[d], fr.e2[d] = e2[d], fr.c[d] = c[d];
     fr.zc = 0.5 * (zlo + zhi);
@@ -212,14 +230,15 @@ __global__ void k_sample_keys(long long K, const double4 *samp, double umax, uns
   idx[k] = static_cast<int>(k);
 }
 
-// Samples and coefficients in key order.
+// Samples, coefficients and (when given) occulter refs in key order.
 __global__ void k_gather_samples(long long K, const int *idx, const double4 *samp, const float2 *coef,
-                                 double4 *ss, float2 *cs) {
+                                 const int4 *refs, double4 *ss, float2 *cs, int4 *rs) {
   const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k >= K) return;
   const int i = idx[k];
   ss[k] = samp[i];
   cs[k] = coef[i];
+  if (refs) rs[k] = refs[i];
 }
 
 // round(a b) for |a b| < 2^22: a b + 1.5 2^23 lies in [2^23, 2^24), where
@@ -230,25 +249,30 @@ __device__ __forceinline__ int round_small(float a, float b) {
 
 // Step 1: samples [b P, b P + P) of the key-ordered samples into facet f's
 // grid, W^3 points each, every contribution times the point's pre-correction
-// pre0[m0] pre1[m1] pre2[m2] = (-1)^m / psi-hat(nu_m).  Shared memory: the
-// box as separate real and imaginary planes of 32-bit fixed-point sums
-// (kBoxCells each), each sample's 3 W kernel weights, its first grid point
-// (3 ints + a spare) and its phased coefficient.  Fixed point because integer
-// adds are native shared-memory atomics (FP32 adds there are compare-and-swap
+// pre0[m0] pre1[m1] pre2[m2] = (-1)^m / psi-hat(nu_m).  With occulter refs
+// (rs non-null) only the samples that see the whole facet (facet_open against
+// its cone) are spread; the direct adjoint takes the others.
+//
+// Shared memory: the box as separate real and imaginary planes of 32-bit
+// fixed-point sums (kBoxCells each), each sample's 3 W kernel weights, its
+// first grid point (3 ints + a spare), its phased coefficient, and each warp's
+// list of the block's samples to spread.  Fixed point because integer adds
+// are native shared-memory atomics (FP32 adds there are compare-and-swap
 // loops): with the scale 4e6 / max_q max(|Re c_q|, |Im c_q|) over the block's
 // samples every contribution is below 2^22 in magnitude (weights <= 1), so it
 // is rounded to an integer by one FMA with 1.5 2^23 (no conversion
 // instruction), and a box point, at most 256 contributions, stays below
 // 2^30.  The step, 2.5e-7 of the block's largest coefficient, is below FP32
-// rounding of the same accumulation (a running sum of several such terms).  Box
-// layout: point (a, b, l) at a P + b n2 + l with n2 odd and P = 7 n2
+// rounding of the same accumulation (a running sum of several such terms).
+// Box layout: point (a, b, l) at a P + b n2 + l with n2 odd and P = 7 n2
 // (mod 32), so lane p = 7 i + j of a warp, which updates row (i, j) of a
 // sample's footprint, hits bank p n2 (mod 32): the 32 lanes of every shared
 // atomic fall in distinct banks.
 __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const double4 *ss, const float2 *cs, int use_off,
-                                                     const FacetFrame *frames, long long f, GridGeom g,
-                                                     const float *pre0, const float *pre1, const float *pre2,
-                                                     float2 *grid, int *status) {
+                                                        const int4 *rs, const float4 *occ32, const float4 *fcones,
+                                                        const FacetFrame *frames, long long f, GridGeom g,
+                                                        const float *pre0, const float *pre1, const float *pre2,
+                                                        float2 *grid, int *status) {
   constexpr int W = kGridW;
   extern __shared__ __align__(16) unsigned char smem[];
   int *box_re = reinterpret_cast<int *>(smem);
@@ -258,13 +282,16 @@ __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const doubl
   float2 *cv = reinterpret_cast<float2 *>(m0s + kSpreadP * 4);       // [P]
   __shared__ int s_lo[3], s_hi[3];
   __shared__ float s_cmag[kSpreadWarps];
-  const int t = threadIdx.x;
+  __shared__ int s_count[kSpreadWarps];
+  __shared__ unsigned char s_list[kSpreadP];                         // per warp: its samples to spread
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if (t < 3) s_lo[t] = INT_MAX, s_hi[t] = INT_MIN;
   __syncthreads();
   const FacetFrame &fr = frames[f];
   const long long k = static_cast<long long>(blockIdx.x) * kSpreadP + t;
-  int ok = 0;
-  if (k < K) {
+  bool ok = k < K && (rs == nullptr || facet_open(rs[k], fcones[f], occ32));
+  float cmag = 0.f;
+  if (ok) {
     const double4 s = ss[k];
     const float2 a = cs[k];
     const double nu[3] = {s.x * fr.e1[0] + s.y * fr.e1[1] + s.z * fr.e1[2],
@@ -278,15 +305,17 @@ __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const doubl
     float2 c = make_float2(a.x * cs_ - a.y * sn, a.x * sn + a.y * cs_);
     if (!isfinite(c.x) || !isfinite(c.y)) {
       atomicOr(status, 4);
-      c = make_float2(0.f, 0.f);
+      ok = false;
     }
     cv[t] = c;
-    ok = 1;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double gp = nu[d] / g.h[d] + 0.5 * g.M[d];       // (nu - nu_0) / h
       const int m = static_cast<int>(ceil(gp - 0.5 * W));
-      if (m < 0 || m + W > g.M[d]) ok = 0;
+      if (m < 0 || m + W > g.M[d]) {
+        if (ok) atomicOr(status, 1);
+        ok = false;
+      }
       m0s[t * 4 + d] = m;
       const float f0 = static_cast<float>(static_cast<double>(m) - gp);
 #pragma unroll
@@ -294,36 +323,29 @@ __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const doubl
         wts[t * kW3 + d * W + i] =
             es_kernel_f((f0 + static_cast<float>(i)) * (2.0f / W), static_cast<float>(kGridBeta));
     }
-    if (!ok) atomicOr(status, 1);
-  } else {
+    if (ok) {
 #pragma unroll
-    for (int i = 0; i < kW3; ++i) wts[t * kW3 + i] = 0.f;
-  }
-  float cmag = 0.f;
-  if (ok) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      atomicMin(&s_lo[d], m0s[t * 4 + d]);
-      atomicMax(&s_hi[d], m0s[t * 4 + d]);
+      for (int d = 0; d < 3; ++d) {
+        atomicMin(&s_lo[d], m0s[t * 4 + d]);
+        atomicMax(&s_hi[d], m0s[t * 4 + d]);
+      }
+      cmag = fmaxf(fabsf(c.x), fabsf(c.y));
     }
-    cmag = fmaxf(fabsf(cv[t].x), fabsf(cv[t].y));
   }
+  // this warp's samples to spread, compacted
+  const unsigned vb = __ballot_sync(0xffffffffu, ok);
+  if (ok) s_list[warp * 32 + __popc(vb & ((1u << lane) - 1u))] = static_cast<unsigned char>(t);
+  if (lane == 0) s_count[warp] = __popc(vb);
   for (int o = 16; o > 0; o >>= 1) cmag = fmaxf(cmag, __shfl_xor_sync(0xffffffffu, cmag, o));
-  if ((t & 31) == 0) s_cmag[t >> 5] = cmag;
+  if (lane == 0) s_cmag[warp] = cmag;
   __syncthreads();
-  if (s_lo[0] == INT_MAX) return;                  // no valid sample in this block (uniform)
+  if (s_lo[0] == INT_MAX) return;                  // nothing to spread in this block (uniform)
   float cmax = 0.f;
 #pragma unroll
   for (int w = 0; w < kSpreadWarps; ++w) cmax = fmaxf(cmax, s_cmag[w]);
-  if (!(cmax > 0.f)) return;                       // nothing to add (uniform)
+  if (!(cmax > 0.f)) return;                       // only zero coefficients (uniform)
   const float fx = 4.0e6f / cmax;                  // fixed-point scale: contributions below 2^22
-  const float inv_fx = cmax * 2.5e-7f;
-  // an invalid sample adds zeros at the box corner
-  if (!ok) {
-    cv[t] = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) m0s[t * 4 + d] = s_lo[d];
-  }
+  const float inv_fx = cmax / 4.0e6f;
   const int lo0 = s_lo[0], lo1 = s_lo[1], lo2 = s_lo[2];
   const long long n0l = s_hi[0] - lo0 + W, n1l = s_hi[1] - lo1 + W;
   const int n2r = s_hi[2] - lo2 + W;
@@ -337,7 +359,7 @@ __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const doubl
     atomicAdd(status + 1, 1);                      // blocks that spread into HBM directly
   }
   __syncthreads();
-  const int lane = t & 31, warp = t >> 5;
+  const int count = s_count[warp];
   const long long M23 = static_cast<long long>(g.M[1]) * g.M[2];
   if (in_box) {
     // this lane's rows of a footprint: p = lane and p = lane + 32 (< W^2)
@@ -346,8 +368,8 @@ __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const doubl
     const bool has_b = pb < W * W;
     const int oa = ia * P + ja * n2, ob = ib * P + jb * n2;
 #pragma unroll 2
-    for (int sidx = 0; sidx < 32; ++sidx) {
-      const int q = warp * 32 + sidx;
+    for (int i = 0; i < count; ++i) {
+      const int q = s_list[warp * 32 + i];
       const int base = (m0s[q * 4] - lo0) * P + (m0s[q * 4 + 1] - lo1) * n2 + (m0s[q * 4 + 2] - lo2);
       const float2 c = cv[q];
       const float *wq = wts + q * kW3;
@@ -376,17 +398,17 @@ __global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const doubl
       }
     }
   } else {
-    for (int sidx = 0; sidx < 32; ++sidx) {
-      const int q = warp * 32 + sidx;
+    for (int i = 0; i < count; ++i) {
+      const int q = s_list[warp * 32 + i];
       const int q0 = m0s[q * 4], q1 = m0s[q * 4 + 1], q2 = m0s[q * 4 + 2];
       const float2 c = cv[q];
       const float *wq = wts + q * kW3;
       for (int p = lane; p < W * W; p += 32) {
-        const int i = p / W, j = p - (p / W) * W;
-        const float wij = wq[i] * wq[W + j];
+        const int ii = p / W, j = p - (p / W) * W;
+        const float wij = wq[ii] * wq[W + j];
         const float vr = c.x * wij, vi = c.y * wij;
-        const float pij = pre0[q0 + i] * pre1[q1 + j];
-        float2 *row = grid + static_cast<long long>(q0 + i) * M23 + static_cast<long long>(q1 + j) * g.M[2] + q2;
+        const float pij = pre0[q0 + ii] * pre1[q1 + j];
+        float2 *row = grid + static_cast<long long>(q0 + ii) * M23 + static_cast<long long>(q1 + j) * g.M[2] + q2;
 #pragma unroll
         for (int l = 0; l < W; ++l) {
           const float wl = wq[2 * W + l] * pij * pre2[q2 + l];
@@ -516,6 +538,37 @@ double kernel_ft(double a, double beta, double f, const std::vector<double> &gx,
   return s * a;
 }
 
+// Occulted plans: of nsub samples (every stride-th) x nF facets, the pairs
+// whose facet is wholly visible (counts[0]) and those neither wholly visible
+// nor wholly hidden (counts[1], the direct kernel's share).
+__global__ void k_count_states(long long nsub, long long stride, const int4 *refs, const float4 *occ32,
+                               const float4 *fcones, long long nF, unsigned long long *counts) {
+  unsigned long long open = 0, mixed = 0;
+  const long long n = nsub * nF;
+  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long k = (i / nF) * stride, f = i - (i / nF) * nF;
+    const int4 rf = refs[k];
+    const float4 cone = fcones[f];
+    if (facet_open(rf, cone, occ32)) {
+      ++open;
+      continue;
+    }
+    bool hidden = false;
+    const int r3[3] = {rf.x, rf.y, rf.z};
+    for (int c = 0; c < 3; ++c) hidden = hidden || (r3[c] >= 0 && cone_state32(cone, occ32[r3[c]]) == 0);
+    if (!hidden) ++mixed;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    open += __shfl_xor_sync(0xffffffffu, open, o);
+    mixed += __shfl_xor_sync(0xffffffffu, mixed, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(counts, open);
+    atomicAdd(counts + 1, mixed);
+  }
+}
+
 // The smallest n >= m with n % 4 == 0 and no prime factor above 7 (FFT-friendly).
 int fft_size(long long m) {
   for (long long n = std::max<long long>(4, (m + 3) / 4 * 4);; n += 4) {
@@ -537,6 +590,10 @@ struct GriddedState {
   bool fft_ok = false;
   FacetFrame *frames = nullptr;
   size_t frames_cap = 0;
+  float4 *fcones = nullptr;        // facet bounding cones (FP32, as the tile cones)
+  size_t fcones_cap = 0;
+  int4 *rs = nullptr;              // occulter refs in key order (occulted plans)
+  size_t rs_cap = 0;
   float *pre = nullptr;            // pre0 | pre1 | pre2
   size_t pre_cap = 0;
   double *tabs = nullptr;          // 3 x kPhiTable
@@ -553,7 +610,7 @@ struct GriddedState {
   size_t cs_cap = 0;
   ~GriddedState() {
     if (fft_ok) cufftDestroy(fft);
-    void *bufs[] = {grid, frames, pre, tabs, status, red, sort, ss, cs};
+    void *bufs[] = {grid, frames, fcones, rs, pre, tabs, status, red, sort, ss, cs};
     for (void *b : bufs)
       if (b) cudaFree(b);
   }
@@ -586,6 +643,9 @@ int cuda_err(cudaError_t e, const char *where) {
 // candidate facet sizes.
 constexpr double kSecPerUpdate = 6.5e-13;
 constexpr double kSecPerCell = 1.6e-11;
+// and per (sample, pixel) pair of a mixed facet left to the direct kernel
+// (tile culling inside the facet included)
+constexpr double kSecPerMixedPair = 3.0e-13;
 
 // Grid shape for targets within |x_d| <= X[d] and |u| <= umax.
 GridGeom grid_geom(const double X_in[3], double umax) {
@@ -615,11 +675,11 @@ double grid_cells(const GridGeom &g) { return static_cast<double>(g.M[0]) * g.M[
 // into X (one device round trip).
 int facet_frames(GriddedState &S, long long J, long long fp, const double4 *pix, cudaStream_t st, double X[3]) {
   const long long nF = (J + fp - 1) / fp;
-  if (!grow(S.frames, S.frames_cap, sizeof(FacetFrame) * nF))
+  if (!grow(S.frames, S.frames_cap, sizeof(FacetFrame) * nF) || !grow(S.fcones, S.fcones_cap, sizeof(float4) * nF))
     return record_error(-3, "viss_adjoint_gridded: device allocation failed (facet frames)");
   cudaError_t e;
   if ((e = cudaMemsetAsync(S.red, 0, 3 * sizeof(unsigned long long), st)) != cudaSuccess) return cuda_err(e, "memset");
-  k_facet_frames<<<static_cast<unsigned>(nF), 256, 0, st>>>(J, fp, pix, S.frames, S.red);
+  k_facet_frames<<<static_cast<unsigned>(nF), 256, 0, st>>>(J, fp, pix, S.frames, S.red, S.fcones);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "frames");
   unsigned long long b[3];
   if ((e = cudaMemcpyAsync(b, S.red, sizeof(b), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -629,9 +689,28 @@ int facet_frames(GriddedState &S, long long J, long long fp, const double4 *pix,
   return 0;
 }
 
+// Shares of wholly visible and of mixed (sample, facet) pairs over the nF
+// facets whose cones are in S.fcones, from up to 2,048 evenly spaced samples.
+int pair_shares(GriddedState &S, long long K, const int4 *refs, const float4 *occ32, long long nF, cudaStream_t st,
+                double &open, double &mixed) {
+  const long long nsub = std::min<long long>(K, 2048), stride = K / nsub;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(S.red + 4, 0, 2 * sizeof(unsigned long long), st)) != cudaSuccess) return cuda_err(e, "memset");
+  k_count_states<<<592, 256, 0, st>>>(nsub, stride, refs, occ32, S.fcones, nF, S.red + 4);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "pair shares");
+  unsigned long long c[2];
+  if ((e = cudaMemcpyAsync(c, S.red + 4, sizeof(c), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_err(e, "read back");
+  const double n = static_cast<double>(nsub) * nF;
+  open = c[0] / n;
+  mixed = c[1] / n;
+  return 0;
+}
+
 // The samples and coefficients in the Morton order of u, into S.ss / S.cs.
-int sort_samples(GriddedState &S, long long K, const double4 *samp, const float2 *coef, double umax,
-                 cudaStream_t st) {
+int sort_samples(GriddedState &S, long long K, const double4 *samp, const float2 *coef, const int4 *refs,
+                 double umax, cudaStream_t st) {
   size_t temp = 0;
   cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<unsigned long long *>(nullptr),
                                                   static_cast<unsigned long long *>(nullptr),
@@ -641,7 +720,7 @@ int sort_samples(GriddedState &S, long long K, const double4 *samp, const float2
   const size_t keys_b = sizeof(unsigned long long) * K, idx_b = sizeof(int) * K;
   const size_t off_idx = 2 * keys_b, off_tmp = (off_idx + 2 * idx_b + 255) / 256 * 256;
   if (!grow(S.sort, S.sort_cap, off_tmp + temp) || !grow(S.ss, S.ss_cap, sizeof(double4) * K) ||
-      !grow(S.cs, S.cs_cap, sizeof(float2) * K))
+      !grow(S.cs, S.cs_cap, sizeof(float2) * K) || (refs && !grow(S.rs, S.rs_cap, sizeof(int4) * K)))
     return record_error(-3, "viss_adjoint_gridded: device allocation failed (sample order)");
   auto *keys = reinterpret_cast<unsigned long long *>(S.sort);
   auto *idx = reinterpret_cast<int *>(S.sort + off_idx);
@@ -651,7 +730,7 @@ int sort_samples(GriddedState &S, long long K, const double4 *samp, const float2
   if ((e = cub::DeviceRadixSort::SortPairs(S.sort + off_tmp, temp, keys, keys + K, idx, idx + K, static_cast<int>(K),
                                            0, 63, st)) != cudaSuccess)
     return cuda_err(e, "sort");
-  k_gather_samples<<<nb, 256, 0, st>>>(K, idx + K, samp, coef, S.ss, S.cs);
+  k_gather_samples<<<nb, 256, 0, st>>>(K, idx + K, samp, coef, refs, S.ss, S.cs, S.rs);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "gather samples");
   return 0;
 }
@@ -666,13 +745,18 @@ int sort_samples(GriddedState &S, long long K, const double4 *samp, const float2
 int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *perm, long long K,
                     const double4 *samp, const float2 *coef, int use_off, long long facet_pix,
                     float scale, float *img, int accumulate, long long max_cells, cudaStream_t st,
-                    int *grid_dims, long long *facet_used, long long *info) {
+                    int *grid_dims, long long *facet_used, long long *info, const int4 *refs,
+                    const float4 *occ32, const float4 **fcones_out) {
   if (K > INT_MAX) return record_error(-1, "viss_adjoint_gridded: more than 2^31 - 1 samples");
+  const bool masked = refs != nullptr;
+  if (masked && facet_pix % kHybridAlign != 0)
+    return record_error(-1, "viss_adjoint_gridded: with occultation, facet_pixels must be a multiple of " +
+                                std::to_string(kHybridAlign));
   if (!*statep) *statep = new GriddedState();
   GriddedState &S = *static_cast<GriddedState *>(*statep);
   if ((!S.tabs && cudaMalloc(&S.tabs, sizeof(double) * 3 * kPhiTable) != cudaSuccess) ||
       (!S.status && cudaMalloc(&S.status, 2 * sizeof(int)) != cudaSuccess) ||
-      (!S.red && cudaMalloc(&S.red, 4 * sizeof(unsigned long long)) != cudaSuccess))
+      (!S.red && cudaMalloc(&S.red, 6 * sizeof(unsigned long long)) != cudaSuccess))
     return record_error(-3, "viss_adjoint_gridded: device allocation failed");
   cudaError_t e;
   if ((e = cudaMemsetAsync(S.red + 3, 0, sizeof(unsigned long long), st)) != cudaSuccess ||
@@ -691,16 +775,23 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
   double X[3];
   long long fp = facet_pix;
   if (fp == 0) {
-    // every candidate's real extents, then the least modelled time
+    // every candidate's real extents (and, with occultation, its share of
+    // wholly visible and of mixed sample-facet pairs), then the least
+    // modelled time
     double best_t = 1e300;
     long long last = 0;
-    for (long long c = 64;; c *= 4) {
+    for (long long c = masked ? kHybridAlign : 64;; c *= 4) {
       if (int s = facet_frames(S, J, c, pix, st, X)) return s;
       last = c;
       const double cells = grid_cells(grid_geom(X, umax));
       if (cells <= static_cast<double>(max_cells)) {
         const double nf = std::ceil(static_cast<double>(J) / c);
-        const double t = nf * (static_cast<double>(K) * kGridW * kGridW * kGridW * kSecPerUpdate + cells * kSecPerCell);
+        double open = 1.0, mixed = 0.0;
+        if (masked)
+          if (int s = pair_shares(S, K, refs, occ32, static_cast<long long>(nf), st, open, mixed)) return s;
+        const double t = nf * (static_cast<double>(K) * open * kGridW * kGridW * kGridW * kSecPerUpdate +
+                               cells * kSecPerCell) +
+                         static_cast<double>(K) * J * mixed * kSecPerMixedPair;
         if (t < best_t) best_t = t, fp = c;
       }
       if (c >= J) break;
@@ -712,6 +803,7 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
     return s;
   }
   if (facet_used) *facet_used = fp;
+  if (fcones_out) *fcones_out = S.fcones;
   const long long nF = (J + fp - 1) / fp;
   // one grid shape for every facet, from the largest extents
   const GridGeom g = grid_geom(X, umax);
@@ -764,7 +856,7 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
     for (int d = 0; d < 3; ++d) S.fft_dims[d] = g.M[d];
   }
   if (cufftSetStream(S.fft, st) != CUFFT_SUCCESS) return record_error(-2, "viss_adjoint_gridded: cufftSetStream failed");
-  if (int s = sort_samples(S, K, samp, coef, umax, st)) return s;
+  if (int s = sort_samples(S, K, samp, coef, refs, umax, st)) return s;
   if ((e = cudaFuncSetAttribute(k_spread, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kSpreadSmem))) != cudaSuccess)
     return cuda_err(e, "spread attributes");
@@ -774,8 +866,9 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
   for (long long f = 0; f < nF; ++f) {
     const long long r0 = f * fp, r1 = std::min(J, r0 + fp);
     if ((e = cudaMemsetAsync(S.grid, 0, sizeof(float2) * cells, st)) != cudaSuccess) return cuda_err(e, "memset");
-    k_spread<<<spread_blocks, kSpreadP, kSpreadSmem, st>>>(K, S.ss, S.cs, use_off, S.frames, f, g, pre0, pre1, pre2,
-                                                           S.grid, S.status);
+    k_spread<<<spread_blocks, kSpreadP, kSpreadSmem, st>>>(K, S.ss, S.cs, use_off, masked ? S.rs : nullptr, occ32,
+                                                           S.fcones, S.frames, f, g, pre0, pre1, pre2, S.grid,
+                                                           S.status);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "spread");
     if (cufftExecC2C(S.fft, reinterpret_cast<cufftComplex *>(S.grid), reinterpret_cast<cufftComplex *>(S.grid),
                      CUFFT_INVERSE) != CUFFT_SUCCESS)

@@ -490,7 +490,7 @@ __device__ __forceinline__ void adj_sample(const double4 &u, double m, const flo
   }
 }
 
-template <int NT, int P, int MINB, bool MASKED, bool FP64>
+template <int NT, int P, int MINB, bool MASKED, bool FP64, bool HYBRID = false>
 __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   static_assert(P == 4 || P == 8, "a warp covers one or two pixel tiles");
   constexpr int kWarpPix = 32 * P;
@@ -520,11 +520,13 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
   }
   // the warp's tile cone(s) in registers, its sub-tile cones in shared memory
   float4 cone0 = make_float4(0.f, 0.f, 1.f, 4.f), cone1 = cone0;
+  float4 fcone = cone0;   // hybrid: the cone of the facet holding this warp's pixels
   if (MASKED && tile_ok) {
     const long long ntiles = p.Jpad / kTilePix;
     cone0 = p.cones[pbase / kTilePix];
     if (P == 8) cone1 = p.cones[pbase / kTilePix + 1];
     if (lane < P) s_sub[warp][lane] = p.cones[ntiles + pbase / 32 + lane];
+    if (HYBRID) fcone = p.fcones[min(pbase / p.facet_pix, p.nfacets - 1)];
   }
   __syncwarp();
 
@@ -608,7 +610,10 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
         st = 0;
         if (lane < gn && tile_ok) {
           const int4 rf = s_refs[buf][g + lane];
-          st = (P == 8) ? sample_state2(rf, cone0, cone1, p.occ32) : sample_state(rf, cone0, p.occ32);
+          // hybrid: a sample that sees the whole facet is the gridded path's
+          st = (HYBRID && facet_open(rf, fcone, p.occ32))
+                   ? 0
+                   : ((P == 8) ? sample_state2(rf, cone0, cone1, p.occ32) : sample_state(rf, cone0, p.occ32));
           if ((st & 3) == 1) {
             int i0, i1, i2;
             const int nr = needed_idx(rf, st, i0, i1, i2);
@@ -782,14 +787,14 @@ int adjoint_ctas_per_sm(int shape, bool fp64) {
   return kAdjShapes[(shape >= 0 && shape < kNumAdjShapes) ? shape : 0].minb;
 }
 
-template <int P, int MINB, bool M, bool F>
+template <int P, int MINB, bool M, bool F, bool H = false>
 static cudaError_t adj_inst(const AdjParams &p, int nchunk, cudaStream_t st) {
   const long long pix_per_cta = static_cast<long long>(kAdjNT / 32) * 32 * P;
   const unsigned gx = static_cast<unsigned>((p.Jpad + pix_per_cta - 1) / pix_per_cta);
   const long long gy = static_cast<long long>(nchunk) * p.channels;
   if (gy > 65535) return cudaErrorInvalidValue;
   dim3 grid(gx, static_cast<unsigned>(gy));
-  k_adjoint<kAdjNT, P, MINB, M, F><<<grid, kAdjNT, 0, st>>>(p);
+  k_adjoint<kAdjNT, P, MINB, M, F, H><<<grid, kAdjNT, 0, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -808,6 +813,19 @@ cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool maske
     case 2: return adj_m<4, 5>(p, nchunk, masked, st);
     case 3: return adj_m<4, 6>(p, nchunk, masked, st);
     default: return adj_m<8, 4>(p, nchunk, masked, st);
+  }
+}
+
+cudaError_t launch_adjoint_hybrid(const AdjParams &p, int shape, int nchunk, cudaStream_t st) {
+  if (p.K <= 0 || p.Jpad <= 0) return cudaSuccess;
+  // a facet must hold whole warp tiles of the widest shape (32 lanes x 8 pixels)
+  if (!p.fcones || p.facet_pix <= 0 || p.facet_pix % (32 * 8) != 0 || p.nfacets <= 0 || !p.refs)
+    return cudaErrorInvalidValue;
+  switch (shape) {
+    case 1: return adj_inst<8, 5, true, false, true>(p, nchunk, st);
+    case 2: return adj_inst<4, 5, true, false, true>(p, nchunk, st);
+    case 3: return adj_inst<4, 6, true, false, true>(p, nchunk, st);
+    default: return adj_inst<8, 4, true, false, true>(p, nchunk, st);
   }
 }
 

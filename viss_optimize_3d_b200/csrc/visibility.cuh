@@ -49,6 +49,11 @@ struct AdjParams {
   long long Kc;                 // samples per channel (even when channels > 1)
   int nchunk;                   // sample chunks per channel (gridDim.y = channels * nchunk)
   int drop_tile;                // test hook: CTA (0, 0) skips this tile's copy (-1: none)
+  // hybrid instance (the occulted gridded adjoint): pairs whose facet the
+  // sample sees wholly (facet_open) are skipped, the gridded path takes them
+  const float4 *fcones = nullptr;   // [nfacets] facet cones
+  long long facet_pix = 0;          // records per facet, a multiple of the warp tile
+  long long nfacets = 0;
 };
 
 // Satellite-formation mode (formation.cu): every sample is a pair a < b of the
@@ -107,6 +112,9 @@ int forward_samples_per_block(int shape, bool fp64);
 int forward_ctas_per_sm(int shape, bool fp64);
 cudaError_t launch_reduce_fwd(long long K, int nchunk, const double2 *part, float2 *V, int acc,
                               cudaStream_t st);
+// The occulted split-precision adjoint without the pairs whose facet is
+// wholly visible to the sample (p.fcones, p.facet_pix, p.nfacets set).
+cudaError_t launch_adjoint_hybrid(const AdjParams &p, int shape, int nchunk, cudaStream_t st);
 cudaError_t launch_adjoint(const AdjParams &p, int shape, int nchunk, bool masked, bool fp64,
                            cudaStream_t st);
 int adjoint_pixels_per_block(int shape, bool fp64);

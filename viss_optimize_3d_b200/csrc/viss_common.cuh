@@ -224,4 +224,14 @@ __device__ __forceinline__ int cone_state32(const float4 &cone, const float4 &q)
   return 1;
 }
 
+// A sample (occulter refs rf, -1 = none) sees every pixel of a cone: each of
+// its rows classifies the cone as wholly visible.  The gridded adjoint's
+// spreading and the direct adjoint's hybrid instance both decide with this
+// one function on the same stored cone and rows, so each (sample, facet) pair
+// is taken by exactly one of them.
+__device__ __forceinline__ bool facet_open(const int4 &rf, const float4 &cone, const float4 *occ32) {
+  return (rf.x < 0 || cone_state32(cone, occ32[rf.x]) == 2) && (rf.y < 0 || cone_state32(cone, occ32[rf.y]) == 2) &&
+         (rf.z < 0 || cone_state32(cone, occ32[rf.z]) == 2);
+}
+
 }  // namespace viss
