@@ -154,28 +154,33 @@ int viss_adjoint(viss_plan *plan, const float *coef, float *image, float scale, 
 int viss_plan_tune(viss_plan *plan, const float *sky, const float *coef, float *V_scratch,
                    float *img_scratch, int flags, int *fwd_shape, int *adj_shape, void *stream);
 
-/* Gridded imaging adjoint, unmasked: the same image as viss_adjoint with
- * VISS_NO_MASK,
- *   image_j = scale * sum_k Re(coef_k exp(+2 pi i (u_k . s_j + off_k))),
- * the adjoint of the reference's noblockage programs (computeC,
- * vissgen3d_noblockage.cu:167-182), through per-facet type-3 NUFFTs.  The
- * plan's pixel records (sorted by a NESTED key) are cut into facets of
- * `facet_pixels` records; 0 picks the size 4^n (n >= 3) with the least
- * modelled time among those whose grid fits, from the facets' measured
- * extents.  Each facet: every sample spread onto a uniform frequency grid in
- * the facet's local frame ("exponential of semicircle" kernel, width 7,
- * oversampling 2), one FFT (cuFFT), interpolation at its pixels.  Relative
- * error ~1e-6.  It pays where pixels are many and baselines short against
- * the pixel spacing (Nside 512 at 1 MHz); at 10 MHz on coarse grids the
- * direct viss_adjoint is faster, and a sky whose grid would exceed 2^29
- * points for every facet size returns VISS_ERR_ARG (so does an explicit
- * facet size whose grid would).  A plan with occulter refs needs VISS_NO_MASK
- * (the occulted adjoint has no gridded form here); one channel; split
- * precision only; VISS_NO_OFFSET and VISS_ACCUMULATE as for viss_adjoint.
- * Allocates its grid (up to 2^29 complex points, 4 GiB), the samples in a
- * sorted copy and the FFT plan on first use and keeps them with the plan;
- * synchronises `stream` several times.  No counterpart in the reference,
- * whose imaging is the direct sum. */
+/* Gridded imaging adjoint: the same image as viss_adjoint (to ~1e-6
+ * relative, split precision),
+ *   image_j = scale * sum_k Re(coef_k exp(+2 pi i (u_k . s_j + off_k))) vis_kj,
+ * through per-facet type-3 NUFFTs.  The plan's pixel records (sorted by a
+ * NESTED key) are cut into facets of `facet_pixels` records; 0 picks the size
+ * 4^n with the least modelled time among those whose grid fits, from the
+ * facets' measured extents.  Each facet: the samples spread onto a uniform
+ * frequency grid in the facet's local frame ("exponential of semicircle"
+ * kernel, width 7, oversampling 2), one FFT (cuFFT, oversampling 1.5),
+ * interpolation at its pixels (width 9).
+ * Unmasked (VISS_NO_MASK, or no occulter refs): computeC of the noblockage
+ * programs (vissgen3d_noblockage.cu:167-182), every sample gridded.
+ * Occulted: computeC of the blockage programs (vissgen3d_blockage.cu:167-192)
+ * as a hybrid: a sample is gridded on the facets it sees wholly (its occulter
+ * rows classify the facet's bounding cone as visible) and every other (sample,
+ * facet) pair goes through the direct kernel, which skips exactly those
+ * pairs; facet_pixels must then be a multiple of 256, and a timed-out wait of
+ * the direct part is reported as for viss_adjoint.
+ * It pays where pixels are many and baselines short against the pixel spacing
+ * (Nside 512 at 1 MHz); on coarse grids or at 10 MHz viss_adjoint is faster,
+ * and a sky whose grid would exceed 2^29 points for every facet size returns
+ * VISS_ERR_ARG (so does an explicit facet size whose grid would).  One
+ * channel; split precision only; VISS_NO_OFFSET and VISS_ACCUMULATE as for
+ * viss_adjoint.  Allocates its grid (up to 2^29 complex points, 4 GiB), the
+ * samples in a sorted copy and the FFT plan on first use and keeps them with
+ * the plan; synchronises `stream` several times.  No counterpart in the
+ * reference, whose imaging is the direct sum. */
 int viss_adjoint_gridded(viss_plan *plan, const float *coef, float *image, float scale, int flags,
                          int64_t facet_pixels, void *stream);
 /* What the last viss_adjoint_gridded on this plan used: facet size, grid
