@@ -57,7 +57,7 @@ int gridded_adjoint(void **state, long long J, const double4 *pix, const int *pe
                     const double4 *samp, const float2 *coef, int use_off, long long facet_pix, float scale,
                     float *img, int accumulate, long long max_cells, cudaStream_t st, int *grid_dims,
                     long long *facet_used, long long *info, const int4 *refs, const float4 *occ32,
-                    const float4 **fcones_out);
+                    const float4 **fcones_out, const unsigned **mixbits_out, long long *mix_words_out);
 void gridded_free(void *state);
 }  // namespace viss
 
@@ -508,7 +508,7 @@ int viss_forward(viss_plan *p, const float *sky, float *V, int flags, void *stre
 // adjoint; facets of facet_pix records, nfacets of them.
 static int adjoint_impl(viss_plan *p, const float *coef, float *image, float scale, int flags,
                         cudaStream_t st, int shape, const float4 *fcones = nullptr, long long facet_pix = 0,
-                        long long nfacets = 0) {
+                        long long nfacets = 0, const unsigned *mixbits = nullptr, long long mix_words = 0) {
   const bool fp64 = (flags & VISS_FP64) != 0;
   const bool masked = p->has_refs && !(flags & VISS_NO_MASK);
   int spc = 0;
@@ -543,6 +543,8 @@ static int adjoint_impl(viss_plan *p, const float *coef, float *image, float sca
     ap.fcones = fcones;
     ap.facet_pix = facet_pix;
     ap.nfacets = nfacets;
+    ap.mixbits = mixbits;
+    ap.mix_words = mix_words;
     VISS_CUDA(viss::launch_adjoint_hybrid(ap, shape, nchunk, st), "viss_adjoint_gridded: direct kernel");
   } else {
     VISS_CUDA(viss::launch_adjoint(ap, shape, nchunk, masked, fp64, st), "viss_adjoint: kernel");
@@ -804,10 +806,13 @@ int viss_adjoint_gridded(viss_plan *p, const float *coef, float *image, float sc
   VISS_CUDA(viss::launch_stage_coef(p->K, p->Kpad, reinterpret_cast<const float2 *>(coef), p->coef, st),
             "viss_adjoint_gridded: coef");
   const float4 *fcones = nullptr;
+  const unsigned *mixbits = nullptr;
+  long long mix_words = 0;
   const int s = viss::gridded_adjoint(&p->gridded, p->J, p->pix, p->perm, p->K, p->samp, p->coef,
                                       (flags & VISS_NO_OFFSET) ? 0 : 1, fp, scale, image,
                                       (flags & VISS_ACCUMULATE) ? 1 : 0, max_cells, st, p->gridded_dims, &fp,
-                                      &info, masked ? p->refs : nullptr, masked ? p->occ32 : nullptr, &fcones);
+                                      &info, masked ? p->refs : nullptr, masked ? p->occ32 : nullptr, &fcones,
+                                      &mixbits, &mix_words);
   p->gridded_facet = fp;
   p->gridded_hbm_blocks = info;
   p->last_stream = st;
@@ -815,7 +820,7 @@ int viss_adjoint_gridded(viss_plan *p, const float *coef, float *image, float sc
   // the occulted adjoint: the direct kernel adds every pair the gridded part
   // left out (facets the sample does not see wholly)
   return adjoint_impl(p, coef, image, scale, (flags & ~VISS_FP64) | VISS_ACCUMULATE, st, p->adj_shape, fcones, fp,
-                      (p->J + fp - 1) / fp);
+                      (p->J + fp - 1) / fp, mixbits, mix_words);
 }
 
 int viss_plan_gridded_info(viss_plan *p, int64_t *facet_pixels, int32_t *grid_dims, int64_t *hbm_blocks) {

@@ -68,6 +68,7 @@ constexpr int kSpreadP = 32 * kSpreadWarps;   // samples per spreading block
 constexpr int kBoxCells = 8192;               // shared-memory box capacity (complex points)
 constexpr int kW3 = 3 * kGridW;               // kernel weights per sample
 constexpr int kHybridAlign = 256;             // occulted plans: facets are whole direct-adjoint warp tiles
+constexpr double kMixBitsMax = 2147483648.0;  // bytes of the mixed-pair bitmask at most
 constexpr size_t kSpreadSmem = 2 * sizeof(float) * kBoxCells + sizeof(float) * kSpreadP * kW3 +
                                sizeof(int) * kSpreadP * 4 + sizeof(float2) * kSpreadP;
 
@@ -569,6 +570,32 @@ __global__ void k_count_states(long long nsub, long long stride, const int4 *ref
   }
 }
 
+// Occulted plans: bit (k mod 32) of mixbits[f * words + k / 32] is set iff
+// sample k (original order) neither sees facet f wholly (facet_open) nor is
+// hidden on all of it (a row classifies the cone as hidden): the pairs the
+// direct kernel must evaluate.  One warp per 32 samples, its rows loaded
+// once and tested against every facet's cone.
+__global__ void k_mixed_bits(long long K, long long nF, long long words, const int4 *refs, const float4 *occ32,
+                             const float4 *fcones, unsigned *mixbits) {
+  const long long w = static_cast<long long>(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+  if (w >= words) return;                                            // uniform over the warp
+  const int lane = threadIdx.x & 31;
+  const long long k = w * 32 + lane;
+  const float4 pass32 = make_float4(0.f, 0.f, 0.f, -4.f);
+  int4 rf = make_int4(-1, -1, -1, -1);
+  if (k < K) rf = refs[k];
+  const float4 r0 = rf.x >= 0 ? occ32[rf.x] : pass32, r1 = rf.y >= 0 ? occ32[rf.y] : pass32,
+               r2 = rf.z >= 0 ? occ32[rf.z] : pass32;
+  for (long long f = 0; f < nF; ++f) {
+    const float4 cone = fcones[f];
+    const int s0 = cone_state32(cone, r0), s1 = cone_state32(cone, r1), s2 = cone_state32(cone, r2);
+    const bool open = (rf.x < 0 || s0 == 2) && (rf.y < 0 || s1 == 2) && (rf.z < 0 || s2 == 2);
+    const bool hidden = (rf.x >= 0 && s0 == 0) || (rf.y >= 0 && s1 == 0) || (rf.z >= 0 && s2 == 0);
+    const unsigned b = __ballot_sync(0xffffffffu, k < K && !open && !hidden);
+    if (lane == 0) mixbits[f * words + w] = b;
+  }
+}
+
 // The smallest n >= m with n % 4 == 0 and no prime factor above 7 (FFT-friendly).
 int fft_size(long long m) {
   for (long long n = std::max<long long>(4, (m + 3) / 4 * 4);; n += 4) {
@@ -594,6 +621,8 @@ struct GriddedState {
   size_t fcones_cap = 0;
   int4 *rs = nullptr;              // occulter refs in key order (occulted plans)
   size_t rs_cap = 0;
+  unsigned *mixbits = nullptr;     // occulted plans: the (sample, facet) pairs left to the direct kernel
+  size_t mixbits_cap = 0;
   float *pre = nullptr;            // pre0 | pre1 | pre2
   size_t pre_cap = 0;
   double *tabs = nullptr;          // 3 x kPhiTable
@@ -610,7 +639,7 @@ struct GriddedState {
   size_t cs_cap = 0;
   ~GriddedState() {
     if (fft_ok) cufftDestroy(fft);
-    void *bufs[] = {grid, frames, fcones, rs, pre, tabs, status, red, sort, ss, cs};
+    void *bufs[] = {grid, frames, fcones, rs, mixbits, pre, tabs, status, red, sort, ss, cs};
     for (void *b : bufs)
       if (b) cudaFree(b);
   }
@@ -746,7 +775,8 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
                     const double4 *samp, const float2 *coef, int use_off, long long facet_pix,
                     float scale, float *img, int accumulate, long long max_cells, cudaStream_t st,
                     int *grid_dims, long long *facet_used, long long *info, const int4 *refs,
-                    const float4 *occ32, const float4 **fcones_out) {
+                    const float4 *occ32, const float4 **fcones_out, const unsigned **mixbits_out,
+                    long long *mix_words_out) {
   if (K > INT_MAX) return record_error(-1, "viss_adjoint_gridded: more than 2^31 - 1 samples");
   const bool masked = refs != nullptr;
   if (masked && facet_pix % kHybridAlign != 0)
@@ -804,6 +834,22 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
   }
   if (facet_used) *facet_used = fp;
   if (fcones_out) *fcones_out = S.fcones;
+  if (mixbits_out) *mixbits_out = nullptr;
+  if (masked) {
+    // the pairs the direct kernel evaluates, once per call (up to 2 GiB of
+    // bits; beyond that the direct kernel classifies each pair itself)
+    const long long nF = (J + fp - 1) / fp, words = (K + 31) / 32;
+    const double bytes = static_cast<double>(nF) * words * sizeof(unsigned);
+    if (bytes <= kMixBitsMax && mixbits_out) {
+      if (!grow(S.mixbits, S.mixbits_cap, static_cast<size_t>(bytes)))
+        return record_error(-3, "viss_adjoint_gridded: device allocation failed (mixed-pair bits)");
+      k_mixed_bits<<<static_cast<unsigned>((words + 7) / 8), 256, 0, st>>>(K, nF, words, refs, occ32, S.fcones,
+                                                                           S.mixbits);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "mixed-pair bits");
+      *mixbits_out = S.mixbits;
+      if (mix_words_out) *mix_words_out = words;
+    }
+  }
   const long long nF = (J + fp - 1) / fp;
   // one grid shape for every facet, from the largest extents
   const GridGeom g = grid_geom(X, umax);

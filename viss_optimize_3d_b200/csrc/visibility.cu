@@ -528,6 +528,9 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
     if (lane < P) s_sub[warp][lane] = p.cones[ntiles + pbase / 32 + lane];
     if (HYBRID) fcone = p.fcones[min(pbase / p.facet_pix, p.nfacets - 1)];
   }
+  // hybrid with the mixed-pair bitmask: this warp's facet row of it
+  const unsigned *mixrow =
+      (HYBRID && p.mixbits) ? p.mixbits + min(pbase / max(p.facet_pix, 1LL), p.nfacets - 1) * p.mix_words : nullptr;
   __syncwarp();
 
   double dacc[P];
@@ -608,10 +611,14 @@ __global__ void __launch_bounds__(NT, MINB) k_adjoint(const AdjParams p) {
       unsigned subm = 0;
       if (MASKED) {
         st = 0;
-        if (lane < gn && tile_ok) {
+        // hybrid: a sample that sees the whole facet is the gridded path's,
+        // one hidden on all of it contributes nothing; with the bitmask both
+        // are skipped without loading their rows (kk + g is a multiple of 32)
+        const bool skip_pair =
+            HYBRID && mixrow && !((__ldg(mixrow + (kk + g) / 32) >> lane) & 1u);
+        if (lane < gn && tile_ok && !skip_pair) {
           const int4 rf = s_refs[buf][g + lane];
-          // hybrid: a sample that sees the whole facet is the gridded path's
-          st = (HYBRID && facet_open(rf, fcone, p.occ32))
+          st = (HYBRID && !mixrow && facet_open(rf, fcone, p.occ32))
                    ? 0
                    : ((P == 8) ? sample_state2(rf, cone0, cone1, p.occ32) : sample_state(rf, cone0, p.occ32));
           if ((st & 3) == 1) {

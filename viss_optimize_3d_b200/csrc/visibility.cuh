@@ -54,6 +54,10 @@ struct AdjParams {
   const float4 *fcones = nullptr;   // [nfacets] facet cones
   long long facet_pix = 0;          // records per facet, a multiple of the warp tile
   long long nfacets = 0;
+  // when set: bit (k mod 32) of mixbits[f * mix_words + k / 32] marks the
+  // pairs (sample k, facet f) to evaluate (all others skipped unclassified)
+  const unsigned *mixbits = nullptr;
+  long long mix_words = 0;
 };
 
 // Satellite-formation mode (formation.cu): every sample is a pair a < b of the
