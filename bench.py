@@ -49,6 +49,8 @@ WORKLOAD_TEXT = {
           "Moon occultation (profiling-size case)",
     "c3_small": "Nside 256 (786,432 px) x 48,600 uvw samples (45 baselines x 1,080 snapshots), "
                 "10 MHz, Moon + Earth occultation (profiling-size case of the headline workload)",
+    "c3_small_1mhz": "Nside 256 (786,432 px) x 48,600 uvw samples (45 baselines x 1,080 snapshots), "
+                     "1 MHz, Moon + Earth occultation (profiling-size case of the gridded adjoint)",
     "c4": "batched: Nside 128 (196,608 px) x 64 channels (1-10 MHz) x 129,600 uvw samples "
           "(45 baselines x 2,880 snapshots), Moon + Earth occultation, spectral index per pixel",
     "c5": "reconstruction: Nside 128 (196,608 px) x 194,400 uvw samples (45 baselines x 4,320 "
@@ -168,6 +170,8 @@ def workload_config(name: str):
     from viss_optimize_3d_b200 import synth
     if name == "c3_small":
         return synth.scaled(synth.CONFIGS["c3_10mhz"], n_snap=1080)
+    if name == "c3_small_1mhz":
+        return synth.scaled(synth.CONFIGS["c3_1mhz"], n_snap=1080)
     return synth.CONFIGS[name]
 
 
@@ -936,7 +940,7 @@ def run_gridded(args):
 
     dev = torch.device("cuda", 0)
     name = args.workload
-    cfg = synth.CONFIGS[name]
+    cfg = workload_config(name)
     obs = synth.make_observation(cfg)
     g = pipeline.upload(obs, cfg.freqs_hz[0], device=dev)
     K, J = g.plan.K, g.plan.J
