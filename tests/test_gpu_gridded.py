@@ -181,3 +181,15 @@ def test_gridded_occulted_counts_exact(c3_small, viss, cuda_device):
         bad = torch.nonzero(n != cols).flatten()
         assert bad.numel() == 0, (facet, bad[:10].tolist(), img[bad[:10]].tolist(), cols[bad[:10]].tolist())
         assert float((img.double() - cols.double()).abs().max()) < 0.3
+
+
+def test_pipeline_observe_gridded(c3_small):
+    """pipeline.observe(gridded=True): the same visibilities, the dirty image
+    through the gridded adjoint within 1e-5 of the direct one."""
+    obs, g = c3_small
+    V, img = pipeline.observe(g)
+    V2, img2 = pipeline.observe(g, gridded=True)
+    assert torch.equal(V, V2)
+    assert rel(img2, img) <= TOL
+    with pytest.raises(ValueError):
+        pipeline.observe(g, fp64=True, gridded=True)

@@ -12,7 +12,9 @@
   --fold-mirrors, each a non-zero exit with a message (no GPU fault involved:
   all are found on the host);
 * --resume: finished days are taken from their image files, a missing one is
-  recomputed bit-identically, the day sum agrees.
+  recomputed bit-identically, the day sum agrees;
+* --gridded: the day images through the gridded adjoint (occulted and
+  unmasked) within 1e-5 of the direct adjoint's.
 """
 import dataclasses
 import json
@@ -194,3 +196,40 @@ def test_resume_skips_finished_days(three_days, tmp_path):
     r = run("vissgen_stream", "--sky", root / "bin" / "sky.vsky", "--days-dir", root / "bin",
             "--resume", ok=False)
     assert r.returncode != 0 and "--resume needs --out-dir" in r.stderr
+
+
+@pytest.fixture(scope="module")
+def low_freq_days(tmp_path_factory, oracle):
+    """Two synthetic days at 0.1 MHz (Nside 16, 6 satellites x 40 snapshots,
+    Moon): baselines short enough against the pixels for the gridded adjoint."""
+    root = tmp_path_factory.mktemp("lowdays")
+    cfg = synth.scaled(synth.CONFIGS["c2"], nside=16, n_snap=40, n_sat=6)
+    th, ph, _ = oracle.pix2ang(cfg.nside)
+    sky = synth.make_observation(cfg).sky.astype(np.float32)
+    dayfile.write_sky(root / "sky.vsky", sky, th, ph)
+    for d in (1, 2):
+        obs = synth.make_observation(dataclasses.replace(cfg, day=float(d - 1)))
+        dayfile.write_day(dayfile.day_path(root, d), dayfile.observation_rows(obs, 1e5), day=d, frequency=1e5)
+    return root, cfg
+
+
+def test_gridded_imaging_in_the_stream(low_freq_days, tmp_path):
+    """--gridded images every day through viss_adjoint_gridded: occulted
+    (hybrid) and unmasked, each day within 1e-5 (rel-L2) of the direct
+    adjoint's image; with --fp64 it is refused before anything runs."""
+    root, cfg = low_freq_days
+    base = ["--sky", root / "sky.vsky", "--days-dir", root, "--days", "2", "--frequency", "1e5"]
+    for blockage in ("1", "0"):
+        outs = {}
+        for mode in ("direct", "gridded"):
+            out = tmp_path / f"{mode}_{blockage}"
+            out.mkdir()
+            extra = ["--gridded"] if mode == "gridded" else []
+            run("vissgen_stream", *base, "--blockage", blockage, "--out-dir", out, *extra)
+            outs[mode] = out
+        for d in (1, 2):
+            a = dayfile.read_image(outs["gridded"] / f"C{d}.vimg")[0].astype(np.float64)
+            b = dayfile.read_image(outs["direct"] / f"C{d}.vimg")[0].astype(np.float64)
+            assert rel_l2(a, b) <= 1e-5, (blockage, d, rel_l2(a, b))
+    r = run("vissgen_stream", *base, "--gridded", "--fp64", ok=False)
+    assert r.returncode != 0 and "--gridded" in r.stderr

@@ -90,16 +90,21 @@ def upload(obs: Observation, f_hz: float, device="cuda", lmn: torch.Tensor | Non
     return GpuObservation(obs, f_hz, lmn, sky, uvw, w, bll, refs, occ, obs.nr(f_hz), plan)
 
 
-def dirty_image(g: GpuObservation, V: torch.Tensor, fp64: bool = False) -> torch.Tensor:
-    """DCF weights and the imaging adjoint for visibilities V."""
+def dirty_image(g: GpuObservation, V: torch.Tensor, fp64: bool = False, gridded: bool = False) -> torch.Tensor:
+    """DCF weights and the imaging adjoint for visibilities V; gridded: through
+    viss_adjoint_gridded (per-facet NUFFTs; split precision only)."""
     gs, _counts, dcf = api.dcf(g.bll, g.nr, multiplicity=2)
     _dg, wt = api.weights(g.w, g.bll, gs, dcf, g.nr)
     coef = api.scale_coef(wt, V)
+    if gridded:
+        if fp64:
+            raise ValueError("the gridded adjoint is split precision only")
+        return g.plan.adjoint_gridded(coef, scale=2.0, mask=g.obs.cfg.imaging_mask)
     return g.plan.adjoint(coef, scale=2.0, fp64=fp64, mask=g.obs.cfg.imaging_mask)
 
 
-def observe(g: GpuObservation, fp64: bool = False):
+def observe(g: GpuObservation, fp64: bool = False, gridded: bool = False):
     """Forward visibilities and the density-compensated dirty image."""
     V = g.plan.forward(g.sky, fp64=fp64)
-    img = dirty_image(g, V, fp64=fp64)
+    img = dirty_image(g, V, fp64=fp64, gridded=gridded)
     return V, img
