@@ -65,7 +65,7 @@ constexpr double kInterpBeta = 0.97 * 3.14159265358979323846 * (1.0 - 1.0 / (2.0
 constexpr int kPhiTable = 8192;           // phi-hat table entries per dimension
 constexpr int kSpreadWarps = 8;
 constexpr int kSpreadP = 32 * kSpreadWarps;   // samples per spreading block
-constexpr int kBoxCells = 8192;               // shared-memory box capacity (complex points)
+constexpr int kBoxCells = 6016;               // shared-memory box capacity (complex points): 3 CTAs per SM
 constexpr int kW3 = 3 * kGridW;               // kernel weights per sample
 constexpr int kHybridAlign = 256;             // occulted plans: facets are whole direct-adjoint warp tiles
 constexpr double kMixBitsMax = 2147483648.0;  // bytes of the mixed-pair bitmask at most
@@ -269,7 +269,7 @@ __device__ __forceinline__ int round_small(float a, float b) {
 // (mod 32), so lane p = 7 i + j of a warp, which updates row (i, j) of a
 // sample's footprint, hits bank p n2 (mod 32): the 32 lanes of every shared
 // atomic fall in distinct banks.
-__global__ void __launch_bounds__(kSpreadP, 2) k_spread(long long K, const double4 *ss, const float2 *cs, int use_off,
+__global__ void __launch_bounds__(kSpreadP, 3) k_spread(long long K, const double4 *ss, const float2 *cs, int use_off,
                                                         const int4 *rs, const float4 *occ32, const float4 *fcones,
                                                         const FacetFrame *frames, long long f, GridGeom g,
                                                         const float *pre0, const float *pre1, const float *pre2,
