@@ -193,3 +193,23 @@ def test_pipeline_observe_gridded(c3_small):
     assert rel(img2, img) <= TOL
     with pytest.raises(ValueError):
         pipeline.observe(g, fp64=True, gridded=True)
+
+
+def test_gridded_repeated_calls_and_restaged_samples(c3_small, cuda_device):
+    """What a call derives from the geometry alone (facet size, |u| bound,
+    sample order, mixed-pair bits) is kept for the next call on the same plan:
+    repeated calls with new coefficients, and a call after the samples were
+    staged again (other baselines), all match the direct adjoint."""
+    obs, g = c3_small
+    plan = api.Plan(g.lmn, g.uvw, None, g.refs, g.occ)
+    for seed in (21, 22, 23):
+        a = _coef(plan.K, cuda_device, seed=seed)
+        for mask in (True, False, True):
+            grid = plan.adjoint_gridded(a, mask=mask)
+            assert rel(grid, plan.adjoint(a, mask=mask)) <= TOL, (seed, mask)
+    first = plan.gridded_info()
+    plan.set_samples(g.uvw * 0.5, None, g.refs, g.occ)        # shorter baselines: another grid
+    a = _coef(plan.K, cuda_device, seed=24)
+    grid = plan.adjoint_gridded(a)
+    assert rel(grid, plan.adjoint(a)) <= TOL
+    assert plan.gridded_info()["grid"] != first["grid"]

@@ -57,7 +57,8 @@ int gridded_adjoint(void **state, long long J, const double4 *pix, const int *pe
                     const double4 *samp, const float2 *coef, int use_off, long long facet_pix, float scale,
                     float *img, int accumulate, long long max_cells, cudaStream_t st, int *grid_dims,
                     long long *facet_used, long long *info, const int4 *refs, const float4 *occ32,
-                    const float4 **fcones_out, const unsigned **mixbits_out, long long *mix_words_out);
+                    const float4 **fcones_out, const unsigned **mixbits_out, long long *mix_words_out,
+                    long long geom_version);
 void gridded_free(void *state);
 }  // namespace viss
 
@@ -179,6 +180,7 @@ struct viss_plan {
   int gridded_dims[3] = {0, 0, 0};
   long long gridded_facet = 0;
   long long gridded_hbm_blocks = 0;
+  long long geom_version = 0;   // bumped by every call that restages pixels or samples
 };
 
 namespace {
@@ -359,6 +361,7 @@ int viss_plan_destroy(viss_plan *p) {
 }
 
 int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *stream) {
+  if (p) ++p->geom_version;
   if (!p || J <= 0 || !lmn) return fail(VISS_ERR_ARG, "viss_plan_set_pixels: bad arguments");
   if (J > (1LL << 31) * viss::kTilePix / 2)
     return fail(VISS_ERR_ARG, "viss_plan_set_pixels: too many pixels");
@@ -392,6 +395,7 @@ int viss_plan_set_pixels(viss_plan *p, int64_t J, const double *lmn, void *strea
 
 int viss_plan_set_samples(viss_plan *p, int64_t K, const double *uvw, const double *off,
                           const int32_t *refs, int64_t G, const double *occ, void *stream) {
+  if (p) ++p->geom_version;
   if (!p || K <= 0 || !uvw) return fail(VISS_ERR_ARG, "viss_plan_set_samples: bad arguments");
   if (refs && (G <= 0 || !occ))
     return fail(VISS_ERR_ARG, "viss_plan_set_samples: refs given without an occulter table");
@@ -610,6 +614,7 @@ int viss_plan_tune(viss_plan *p, const float *sky, const float *coef, float *V_s
 }
 
 int viss_plan_set_channels(viss_plan *p, int channels) {
+  if (p) ++p->geom_version;
   if (!p || channels < 1) return fail(VISS_ERR_ARG, "viss_plan_set_channels: bad arguments");
   if (p->K <= 0) return fail(VISS_ERR_STATE, "viss_plan_set_channels: samples not set");
   if (p->K % channels != 0)
@@ -812,7 +817,7 @@ int viss_adjoint_gridded(viss_plan *p, const float *coef, float *image, float sc
                                       (flags & VISS_NO_OFFSET) ? 0 : 1, fp, scale, image,
                                       (flags & VISS_ACCUMULATE) ? 1 : 0, max_cells, st, p->gridded_dims, &fp,
                                       &info, masked ? p->refs : nullptr, masked ? p->occ32 : nullptr, &fcones,
-                                      &mixbits, &mix_words);
+                                      &mixbits, &mix_words, p->geom_version);
   p->gridded_facet = fp;
   p->gridded_hbm_blocks = info;
   p->last_stream = st;

@@ -231,6 +231,12 @@ __global__ void k_sample_keys(long long K, const double4 *samp, double umax, uns
   idx[k] = static_cast<int>(k);
 }
 
+// Coefficients alone in key order (the samples' order kept from an earlier call).
+__global__ void k_gather_coef(long long K, const int *idx, const float2 *coef, float2 *cs) {
+  const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k < K) cs[k] = coef[idx[k]];
+}
+
 // Samples, coefficients and (when given) occulter refs in key order.
 __global__ void k_gather_samples(long long K, const int *idx, const double4 *samp, const float2 *coef,
                                  const int4 *refs, double4 *ss, float2 *cs, int4 *rs) {
@@ -639,6 +645,12 @@ struct GriddedState {
   size_t ss_cap = 0;
   float2 *cs = nullptr;            // coefficients in key order
   size_t cs_cap = 0;
+  // what the last successful call derived from the plan's geometry alone (the
+  // |u| bound, the facet size and extents, the sample order, the mixed-pair
+  // bits), reused while the plan's geometry version and the request match
+  long long cache_version = -1, cache_request = -1, cache_fp = 0, cache_words = 0;
+  bool cache_masked = false, cache_mix = false;
+  double cache_umax = 0, cache_X[3] = {0, 0, 0};
   ~GriddedState() {
     if (fft_ok) cufftDestroy(fft);
     void *bufs[] = {grid, frames, fcones, rs, mixbits, pre, tabs, status, red, sort, ss, cs};
@@ -778,7 +790,7 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
                     float scale, float *img, int accumulate, long long max_cells, cudaStream_t st,
                     int *grid_dims, long long *facet_used, long long *info, const int4 *refs,
                     const float4 *occ32, const float4 **fcones_out, const unsigned **mixbits_out,
-                    long long *mix_words_out) {
+                    long long *mix_words_out, long long geom_version) {
   if (K > INT_MAX) return record_error(-1, "viss_adjoint_gridded: more than 2^31 - 1 samples");
   const bool masked = refs != nullptr;
   if (masked && facet_pix % kHybridAlign != 0)
@@ -794,19 +806,26 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
   if ((e = cudaMemsetAsync(S.red + 3, 0, sizeof(unsigned long long), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(S.status, 0, 2 * sizeof(int), st)) != cudaSuccess)
     return cuda_err(e, "memset");
-  k_max_unorm<<<static_cast<unsigned>((K + 255) / 256), 256, 0, st>>>(K, samp, S.red + 3);
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "max |u|");
-  unsigned long long ub = 0;
-  if ((e = cudaMemcpyAsync(&ub, S.red + 3, sizeof(ub), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(st)) != cudaSuccess)
-    return cuda_err(e, "read back");
-  double umax;
-  std::memcpy(&umax, &ub, sizeof(umax));
-  if (!std::isfinite(umax)) return record_error(-5, "viss_adjoint_gridded: non-finite uvw");
+  const bool cached = geom_version >= 0 && S.cache_version == geom_version && S.cache_request == facet_pix &&
+                      S.cache_masked == masked;
+  S.cache_version = -1;   // set again only when this call succeeds
+  double umax = S.cache_umax;
+  if (!cached) {
+    k_max_unorm<<<static_cast<unsigned>((K + 255) / 256), 256, 0, st>>>(K, samp, S.red + 3);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "max |u|");
+    unsigned long long ub = 0;
+    if ((e = cudaMemcpyAsync(&ub, S.red + 3, sizeof(ub), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return cuda_err(e, "read back");
+    std::memcpy(&umax, &ub, sizeof(umax));
+    if (!std::isfinite(umax)) return record_error(-5, "viss_adjoint_gridded: non-finite uvw");
+  }
 
-  double X[3];
-  long long fp = facet_pix;
-  if (fp == 0) {
+  double X[3] = {S.cache_X[0], S.cache_X[1], S.cache_X[2]};
+  long long fp = cached ? S.cache_fp : facet_pix;
+  if (cached) {
+    // frames, cones, sorted samples and mixed-pair bits are those of the last call
+  } else if (fp == 0) {
     // every candidate's real extents (and, with occultation, its share of
     // wholly visible and of mixed sample-facet pairs), then the least
     // modelled time
@@ -837,10 +856,16 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
   if (facet_used) *facet_used = fp;
   if (fcones_out) *fcones_out = S.fcones;
   if (mixbits_out) *mixbits_out = nullptr;
-  if (masked) {
-    // the pairs the direct kernel evaluates, once per call (up to 2 GiB of
-    // bits; beyond that the direct kernel classifies each pair itself)
-    const long long nF = (J + fp - 1) / fp, words = (K + 31) / 32;
+  bool mix_ok = false;
+  const long long words = (K + 31) / 32;
+  if (masked && cached) {
+    mix_ok = S.cache_mix;
+    if (mix_ok && mixbits_out) *mixbits_out = S.mixbits;
+    if (mix_ok && mix_words_out) *mix_words_out = S.cache_words;
+  } else if (masked) {
+    // the pairs the direct kernel evaluates, once per geometry (up to 2 GiB
+    // of bits; beyond that the direct kernel classifies each pair itself)
+    const long long nF = (J + fp - 1) / fp;
     const double bytes = static_cast<double>(nF) * words * sizeof(unsigned);
     if (bytes <= kMixBitsMax && mixbits_out) {
       if (!grow(S.mixbits, S.mixbits_cap, static_cast<size_t>(bytes)))
@@ -850,6 +875,7 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
       if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "mixed-pair bits");
       *mixbits_out = S.mixbits;
       if (mix_words_out) *mix_words_out = words;
+      mix_ok = true;
     }
   }
   const long long nF = (J + fp - 1) / fp;
@@ -904,7 +930,13 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
     for (int d = 0; d < 3; ++d) S.fft_dims[d] = g.M[d];
   }
   if (cufftSetStream(S.fft, st) != CUFFT_SUCCESS) return record_error(-2, "viss_adjoint_gridded: cufftSetStream failed");
-  if (int s = sort_samples(S, K, samp, coef, refs, umax, st)) return s;
+  if (cached) {
+    const int *idx = reinterpret_cast<const int *>(S.sort + 2 * sizeof(unsigned long long) * K) + K;
+    k_gather_coef<<<static_cast<unsigned>((K + 255) / 256), 256, 0, st>>>(K, idx, coef, S.cs);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "gather coefficients");
+  } else if (int s = sort_samples(S, K, samp, coef, refs, umax, st)) {
+    return s;
+  }
   if ((e = cudaFuncSetAttribute(k_spread, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kSpreadSmem))) != cudaSuccess)
     return cuda_err(e, "spread attributes");
@@ -933,6 +965,14 @@ int gridded_adjoint(void **statep, long long J, const double4 *pix, const int *p
   if (info) info[0] = status[1];
   if (status[0] & 4) return record_error(-5, "viss_adjoint_gridded: non-finite coefficients");
   if (status[0]) return record_error(-2, "viss_adjoint_gridded: a kernel footprint left the grid (internal error)");
+  S.cache_version = geom_version;
+  S.cache_request = facet_pix;
+  S.cache_masked = masked;
+  S.cache_fp = fp;
+  S.cache_umax = umax;
+  for (int d = 0; d < 3; ++d) S.cache_X[d] = X[d];
+  S.cache_mix = mix_ok;
+  S.cache_words = words;
   return 0;
 }
 
