@@ -79,3 +79,21 @@ def test_reference_arm_steps_are_bounded_samples(bench):
     assert r["config"] == bench.bench_config(args, 12288, 10080, 1)
     assert r["cpu_baseline"]["kind"] == "port" and r["e2e"]["h2d_bytes_per_step"] == 0
     assert bench.run_reference(args, 1, 2) is None      # only rank 0 prints
+
+
+def test_workloads_and_traffic_key(bench):
+    """Every workload name resolves to a configuration (the profiling-size
+    gridded case: Nside 256 x 48,600 samples at 1 MHz); the traffic record is
+    keyed on the measured kernels' translation units only, so a change to
+    another source (the gridded adjoint's) leaves it valid."""
+    for name in bench.WORKLOAD_TEXT:
+        if name in ("c4", "c5", "stream"):
+            continue
+        cfg = bench.workload_config(name)
+        assert cfg.nside > 0 and cfg.n_samples > 0, name
+    small = bench.workload_config("c3_small_1mhz")
+    assert (small.nside, small.n_samples, small.freqs_hz) == (256, 48600, (1e6,))
+    assert "gridded.cu" not in bench.TRAFFIC_KERNEL_SOURCES
+    assert {"visibility.cu", "formation.cu"} <= set(bench.TRAFFIC_KERNEL_SOURCES)
+    a = bench.kernel_sources_sha()
+    assert a == bench.kernel_sources_sha() and len(a) == 64

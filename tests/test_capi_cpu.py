@@ -30,6 +30,8 @@ def test_version_and_status_strings(viss):
     lambda L: L.viss_plan_create(None),
     lambda L: L.viss_forward(None, None, None, 0, None),
     lambda L: L.viss_adjoint(None, None, None, 1.0, 0, None),
+    lambda L: L.viss_adjoint_gridded(None, None, None, 1.0, 0, 0, None),
+    lambda L: L.viss_plan_gridded_info(None, None, None, None),
     lambda L: L.viss_dcf(10, None, 5, 1, None, None, None, None),
     lambda L: L.viss_dcf(10, C.c_void_p(16), 0, 1, None, None, C.c_void_p(16), None),  # nr 0
     lambda L: L.viss_occulters(3, C.c_void_p(16), -1.0, 0, 0.0, C.c_void_p(16), None),
